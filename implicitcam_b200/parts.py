@@ -1,0 +1,299 @@
+"""Seeded synthetic parts, built as closed B-rep solids (``solid.SolidBuilder``).
+
+- ``can``: the reference's own test solid, a cylinder r 3 from z 0 to 5
+  (crates/icam-core/src/solid3.rs:2009-2041);
+- ``bump_box``: the reference's 10 x 10 box with a biquadratic B-spline top
+  (solid3.rs:2092-2147);
+- ``block_with_hole``: a 100 x 60 x 40 mm block minus a 20 mm through-hole along z
+  at its centre (6 planes + 1 cylinder);
+- ``freeform_top``: a 120 x 120 x 50 mm block whose top face is a clamped bicubic
+  rational B-spline with 16 x 16 control points, heights 50 mm plus 8 seeded
+  Gaussian bumps, weights in [0.8, 1.2].
+
+Random numbers come from the reference checkers' xorshift64 generator
+(crates/icam-check/src/exact_check.rs:45-52) seeded through splitmix64, so that
+seed 0 is usable.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .solid import (
+    CYLINDER, NURBS, PLANE, Frame, SolidBuilder, arc_pcurve, elevate_to_cubic, line_pcurve,
+    surface_spans,
+)
+
+TAU = 2.0 * math.pi
+MASK = (1 << 64) - 1
+
+
+class Rng:
+    """xorshift64 (exact_check.rs:45-52), seeded by splitmix64(seed)."""
+
+    def __init__(self, seed: int):
+        z = (seed + 0x9E3779B97F4A7C15) & MASK
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & MASK
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & MASK
+        z ^= z >> 31
+        self.s = z or 0x2545F4914F6CDD1D
+
+    def next(self) -> int:
+        x = self.s
+        x ^= (x << 13) & MASK
+        x ^= x >> 7
+        x ^= (x << 17) & MASK
+        self.s = x
+        return x
+
+    def uniform(self, a=0.0, b=1.0) -> float:
+        return a + (b - a) * ((self.next() >> 11) * (1.0 / (1 << 53)))
+
+
+def _pad(lo, hi, frac=0.05):
+    lo, hi = np.asarray(lo, float), np.asarray(hi, float)
+    p = frac * (hi - lo) + 1e-9 * (np.abs(hi) + np.abs(lo)) + 1e-6
+    return lo - p, hi + p
+
+
+class _Plane:
+    """A planar face's frame and the map of 3D edges into its (u, v)."""
+
+    def __init__(self, frame: Frame):
+        self.fr = frame
+
+    def uv(self, p):
+        return self.fr.local(p)[:2]
+
+    def pcurve(self, b: SolidBuilder, ei, rev):
+        e = b.edges[ei]
+        if e.kind == 0:
+            a, c = self.uv(list(e.a)), self.uv(list(e.b))
+            pcs = line_pcurve(a, c)
+        elif e.kind == 1:
+            af = Frame(list(e.f.o), list(e.f.z), list(e.f.x))
+
+            def to_uv(q2):
+                return self.uv(af.world([q2[0], q2[1], 0.0]))
+
+            pcs = arc_pcurve([0.0, 0.0], e.r, e.t0, e.sweep, to_uv)
+        else:
+            pcs = []
+            deg = e.degree
+            for k in range(e.n_pieces):
+                p = b.cpieces[e.first_piece + k]
+                hom = []
+                for q in p:
+                    w = q[3]
+                    xyz = q[:3] / w
+                    u, v = self.uv(xyz)
+                    hom.append([u * w, v * w, w])
+                pcs.append(elevate_to_cubic(np.array(hom)) if deg < 3 else np.array(hom))
+        if rev:
+            pcs = [pc[::-1].copy() for pc in pcs[::-1]]
+        return pcs
+
+    def domain(self, b: SolidBuilder, uses):
+        pts = []
+        for ei, rev in uses:
+            for pc in self.pcurve(b, ei, rev):
+                pts.extend(pc[:, :2] / pc[:, 2:3])
+        pts = np.array(pts)
+        return _pad(pts.min(0), pts.max(0))
+
+
+def _plane_face(b: SolidBuilder, frame: Frame, sense, loops):
+    """loops: [[(edge, rev), ...], ...]"""
+    pl = _Plane(frame)
+    lo, hi = pl.domain(b, [u for lp in loops for u in lp])
+    f = b.face(PLANE, sense, frame, lo=lo, hi=hi)
+    for lp in loops:
+        b.loop(f, [(ei, rev, pl.pcurve(b, ei, rev)) for ei, rev in lp])
+    return f
+
+
+def can(r=3.0, height=5.0):
+    """The reference test's can (solid3.rs:2009-2041): two planes, one cylinder,
+    two circles, one seam."""
+    b = SolidBuilder(tol=1e-9)
+    z, x = [0, 0, 1], [1, 0, 0]
+    f0 = Frame([0, 0, 0], z, x)
+    f1 = Frame([0, 0, height], z, x)
+    va = b.vertex([r, 0, 0])
+    vb = b.vertex([r, 0, height])
+    c0 = b.arc(f0, r, 0.0, TAU, va, va)
+    c1 = b.arc(f1, r, 0.0, TAU, vb, vb)
+    seam = b.line(va, vb)
+    _plane_face(b, f0, -1, [[(c0, True)]])
+    _plane_face(b, f1, +1, [[(c1, False)]])
+    lo, hi = _pad([0.0, 0.0], [TAU, height])
+    cyl = b.face(CYLINDER, +1, f0, a=r, lo=[0.0, lo[1]], hi=[TAU, hi[1]], period=[TAU, 0.0])
+    b.loop(cyl, [
+        (c0, False, line_pcurve([0.0, 0.0], [TAU, 0.0])),
+        (seam, False, None),
+        (c1, True, line_pcurve([TAU, height], [0.0, height])),
+        (seam, True, None),
+    ])
+    return b
+
+
+def block_with_hole(size=(100.0, 60.0, 40.0), center=(50.0, 30.0), r=10.0):
+    """A block [0,X]x[0,Y]x[0,Z] minus a through-hole of radius r along z."""
+    X, Y, Z = size
+    b = SolidBuilder(tol=1e-9)
+    c = {}
+    for i, x in enumerate((0.0, X)):
+        for j, y in enumerate((0.0, Y)):
+            for k, zz in enumerate((0.0, Z)):
+                c[i, j, k] = b.vertex([x, y, zz])
+    L = lambda p, q: b.line(c[p], c[q])  # noqa: E731
+    eb = [L((0, 0, 0), (1, 0, 0)), L((1, 0, 0), (1, 1, 0)), L((1, 1, 0), (0, 1, 0)), L((0, 1, 0), (0, 0, 0))]
+    et = [L((0, 0, 1), (1, 0, 1)), L((1, 0, 1), (1, 1, 1)), L((1, 1, 1), (0, 1, 1)), L((0, 1, 1), (0, 0, 1))]
+    ev = {ij: L((*ij, 0), (*ij, 1)) for ij in ((0, 0), (1, 0), (1, 1), (0, 1))}
+    cx, cy = center
+    va = b.vertex([cx + r, cy, 0.0])
+    vb = b.vertex([cx + r, cy, Z])
+    fz0 = Frame([cx, cy, 0.0], [0, 0, 1], [1, 0, 0])
+    fz1 = Frame([cx, cy, Z], [0, 0, 1], [1, 0, 0])
+    c0 = b.arc(fz0, r, 0.0, TAU, va, va)
+    c1 = b.arc(fz1, r, 0.0, TAU, vb, vb)
+    seam = b.line(va, vb)
+    # bottom (outward -z): clockwise in xy, the hole counterclockwise
+    _plane_face(b, Frame([0, 0, 0], [0, 0, 1], [1, 0, 0]), -1,
+                [[(eb[3], True), (eb[2], True), (eb[1], True), (eb[0], True)], [(c0, False)]])
+    # top (outward +z)
+    _plane_face(b, Frame([0, 0, Z], [0, 0, 1], [1, 0, 0]), +1,
+                [[(et[0], False), (et[1], False), (et[2], False), (et[3], False)], [(c1, True)]])
+    # front y = 0 (outward -y): local (x, z)
+    _plane_face(b, Frame([0, 0, 0], [0, -1, 0], [1, 0, 0]), +1,
+                [[(eb[0], False), (ev[1, 0], False), (et[0], True), (ev[0, 0], True)]])
+    # right x = X (outward +x): local (y, z)
+    _plane_face(b, Frame([X, 0, 0], [1, 0, 0], [0, 1, 0]), +1,
+                [[(eb[1], False), (ev[1, 1], False), (et[1], True), (ev[1, 0], True)]])
+    # back y = Y (outward +y): local (X - x, z)
+    _plane_face(b, Frame([X, Y, 0], [0, 1, 0], [-1, 0, 0]), +1,
+                [[(eb[2], False), (ev[0, 1], False), (et[2], True), (ev[1, 1], True)]])
+    # left x = 0 (outward -x): local (Y - y, z)
+    _plane_face(b, Frame([0, Y, 0], [-1, 0, 0], [0, -1, 0]), +1,
+                [[(eb[3], False), (ev[0, 0], False), (et[3], True), (ev[0, 1], True)]])
+    # the hole's wall: outward toward the axis (sense -1), (angle, height)
+    lo, hi = _pad([0.0, 0.0], [TAU, Z])
+    cyl = b.face(CYLINDER, -1, fz0, a=r, lo=[0.0, lo[1]], hi=[TAU, hi[1]], period=[TAU, 0.0])
+    b.loop(cyl, [
+        (c1, False, line_pcurve([0.0, Z], [TAU, Z])),
+        (seam, True, None),
+        (c0, True, line_pcurve([TAU, 0.0], [0.0, 0.0])),
+        (seam, False, None),
+    ])
+    return b
+
+
+def _boundary_pieces(patches, side):
+    """The Bezier pieces of a surface's boundary iso-curve, in increasing parameter:
+    side 'u0', 'u1' (u fixed, along v) or 'v0', 'v1' (v fixed, along u)."""
+    nsu, nsv = patches.shape[:2]
+    if side == "u0":
+        return [patches[0, j, 0, :, :].copy() for j in range(nsv)]
+    if side == "u1":
+        return [patches[nsu - 1, j, -1, :, :].copy() for j in range(nsv)]
+    if side == "v0":
+        return [patches[i, 0, :, 0, :].copy() for i in range(nsu)]
+    return [patches[i, nsv - 1, :, -1, :].copy() for i in range(nsu)]
+
+
+def _nurbs_box(b: SolidBuilder, du, dv, ku, kv, net_h, X, Y, top_sense=+1):
+    """A block [0,X]x[0,Y]x[0,top] whose top face is the given clamped rational
+    B-spline (u along x, v along y; its boundary iso-curves lie in the four side
+    planes), four side planes and a bottom plane."""
+    patches, ub, vb = surface_spans(du, dv, ku, kv, net_h)
+    corner = lambda h: h[:3] / h[3]  # noqa: E731
+    P = np.asarray(net_h)
+    c = {}
+    for i, x in enumerate((0.0, X)):
+        for j, y in enumerate((0.0, Y)):
+            c[i, j, 0] = b.vertex([x, y, 0.0])
+            c[i, j, 1] = b.vertex(corner(P[-1 if i else 0, -1 if j else 0]))
+    L = lambda p, q: b.line(c[p], c[q])  # noqa: E731
+    eb = [L((0, 0, 0), (1, 0, 0)), L((1, 0, 0), (1, 1, 0)), L((1, 1, 0), (0, 1, 0)), L((0, 1, 0), (0, 0, 0))]
+    ev = {ij: L((*ij, 0), (*ij, 1)) for ij in ((0, 0), (1, 0), (1, 1), (0, 1))}
+    # top edges, stored in increasing surface parameter
+    s_v0 = b.spline(_boundary_pieces(patches, "v0"), c[0, 0, 1], c[1, 0, 1])  # y = 0, along x
+    s_u1 = b.spline(_boundary_pieces(patches, "u1"), c[1, 0, 1], c[1, 1, 1])  # x = X, along y
+    s_v1 = b.spline(_boundary_pieces(patches, "v1"), c[0, 1, 1], c[1, 1, 1])  # y = Y, along x
+    s_u0 = b.spline(_boundary_pieces(patches, "u0"), c[0, 0, 1], c[0, 1, 1])  # x = 0, along y
+    u0, u1, v0, v1 = ub[0], ub[-1], vb[0], vb[-1]
+    top = b.face(NURBS, top_sense, lo=[u0, v0], hi=[u1, v1], nurbs=(patches, ub, vb))
+    b.loop(top, [
+        (s_v0, False, line_pcurve([u0, v0], [u1, v0])),
+        (s_u1, False, line_pcurve([u1, v0], [u1, v1])),
+        (s_v1, True, line_pcurve([u1, v1], [u0, v1])),
+        (s_u0, True, line_pcurve([u0, v1], [u0, v0])),
+    ])
+    _plane_face(b, Frame([0, 0, 0], [0, 0, 1], [1, 0, 0]), -1,
+                [[(eb[3], True), (eb[2], True), (eb[1], True), (eb[0], True)]])
+    _plane_face(b, Frame([0, 0, 0], [0, -1, 0], [1, 0, 0]), +1,
+                [[(eb[0], False), (ev[1, 0], False), (s_v0, True), (ev[0, 0], True)]])
+    _plane_face(b, Frame([X, 0, 0], [1, 0, 0], [0, 1, 0]), +1,
+                [[(eb[1], False), (ev[1, 1], False), (s_u1, True), (ev[1, 0], True)]])
+    _plane_face(b, Frame([X, Y, 0], [0, 1, 0], [-1, 0, 0]), +1,
+                [[(eb[2], False), (ev[0, 1], False), (s_v1, False), (ev[1, 1], True)]])
+    _plane_face(b, Frame([0, Y, 0], [-1, 0, 0], [0, -1, 0]), +1,
+                [[(eb[3], False), (ev[0, 0], False), (s_u0, False), (ev[0, 1], True)]])
+    return b
+
+
+def bump_box():
+    """The reference test's bump box (solid3.rs:2092-2147): a 10 x 10 box whose top
+    is a biquadratic B-spline over the square, z(5i, 5j) control heights zc."""
+    zc = [[5.0, 5.0, 5.0], [7.0, 9.0, 5.0], [5.0, 6.0, 5.0]]
+    net = np.array([[[5.0 * i, 5.0 * j, zc[i][j], 1.0] for j in range(3)] for i in range(3)])
+    k = [0.0, 0.0, 0.0, 1.0, 1.0, 1.0]
+    b = SolidBuilder(tol=1e-9)
+    return _nurbs_box(b, 2, 2, k, k, net, 10.0, 10.0)
+
+
+def bump_box_top(x, y):
+    """The bump box's top height z = S(x, y) (its B-spline in closed form)."""
+    zc = [[5.0, 5.0, 5.0], [7.0, 9.0, 5.0], [5.0, 6.0, 5.0]]
+
+    def bern(t):
+        return [(1 - t) ** 2, 2 * t * (1 - t), t * t]
+
+    bu, bv = bern(x / 10.0), bern(y / 10.0)
+    return sum(bu[i] * bv[j] * zc[i][j] for i in range(3) for j in range(3))
+
+
+def freeform_top(seed=0, n=16, size=120.0, base=50.0, bumps=8):
+    """A size x size x base block whose top is a clamped bicubic rational B-spline:
+    n x n control points on a uniform grid, heights base + the sum of `bumps`
+    Gaussians (amplitude U[2,6] mm, sigma U[8,25] mm, centres U[0,size]^2), weights
+    U[0.8,1.2], uniform interior knots (n - 3 spans each way)."""
+    rng = Rng(seed)
+    g = []
+    for _ in range(bumps):
+        a = rng.uniform(2.0, 6.0)
+        s = rng.uniform(8.0, 25.0)
+        cx = rng.uniform(0.0, size)
+        cy = rng.uniform(0.0, size)
+        g.append((a, s, cx, cy))
+    step = size / (n - 1)
+    net = np.zeros((n, n, 4))
+    for i in range(n):
+        for j in range(n):
+            x, y = step * i, step * j
+            z = base + sum(a * math.exp(-((x - cx) ** 2 + (y - cy) ** 2) / (2 * s * s)) for a, s, cx, cy in g)
+            w = rng.uniform(0.8, 1.2)
+            net[i, j] = [x * w, y * w, z * w, w]
+    spans = n - 3
+    knots = [0.0] * 4 + [k / spans for k in range(1, spans)] + [1.0] * 4
+    b = SolidBuilder(tol=1e-9)
+    return _nurbs_box(b, 3, 3, knots, knots, net, size, size)
+
+
+CONFIGS = {
+    "can": can,
+    "bump_box": bump_box,
+    "block_with_hole": block_with_hole,
+    "freeform_top": freeform_top,
+}
