@@ -1,0 +1,516 @@
+// The C ABI of include/icam_cuda.h: pack creation and upload, point and brick reads,
+// and the level bake of the brick cache, all on one CUDA stream per pack.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cub/cub.cuh>
+
+#include "../../include/icam_cuda.h"
+#include "kernels.h"
+#include "pack_build.h"
+
+using namespace icam;
+
+struct IcamPack {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  HostPack host;
+  DPack dev{};
+  std::vector<void*> owned;  // the pack's device arrays
+  std::vector<int32_t> leaves_host;
+  int32_t* leaves = nullptr;
+  // scratch, grown on demand
+  struct Buf {
+    void* p = nullptr;
+    size_t n = 0;
+  };
+  Buf scratch[16];
+  std::string err;
+  unsigned long long* d_stats = nullptr;
+  const uint32_t* last_map = nullptr;
+  const uint32_t* last_atlas = nullptr;
+};
+
+namespace {
+
+int fail(IcamPack* pk, int code, const std::string& msg) {
+  if (pk) pk->err = msg;
+  return code;
+}
+
+#define CK(call)                                                                              \
+  do {                                                                                        \
+    cudaError_t e_ = (call);                                                                  \
+    if (e_ != cudaSuccess) return fail(pk, ICAM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+template <class T>
+int upload(IcamPack* pk, const std::vector<T>& v, const T** out) {
+  if (v.empty()) {
+    *out = nullptr;
+    return ICAM_OK;
+  }
+  void* d = nullptr;
+  CK(cudaMalloc(&d, v.size() * sizeof(T)));
+  pk->owned.push_back(d);
+  CK(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, pk->stream));
+  *out = static_cast<const T*>(d);
+  return ICAM_OK;
+}
+
+// A scratch buffer of at least `bytes`, slot k.
+int scratch(IcamPack* pk, int k, size_t bytes, void** out) {
+  auto& b = pk->scratch[k];
+  if (b.n < bytes) {
+    if (b.p) CK(cudaFree(b.p));
+    b.p = nullptr;
+    b.n = 0;
+    size_t want = std::max(bytes, size_t(1) << 16);
+    CK(cudaMalloc(&b.p, want));
+    b.n = want;
+  }
+  *out = b.p;
+  return ICAM_OK;
+}
+
+int grid_for(int64_t n, int threads) {
+  int64_t g = (n + threads - 1) / threads;
+  return int(std::max<int64_t>(1, std::min<int64_t>(g, 148 * 32)));
+}
+
+}  // namespace
+
+extern "C" {
+
+int icam_pack_create(const IcamSolidDesc* solid, const IcamPackOptions* opt, IcamPack** out, char* err,
+                     size_t errlen) {
+  auto report = [&](const std::string& m) {
+    if (err && errlen) {
+      std::snprintf(err, errlen, "%s", m.c_str());
+    }
+  };
+  if (!solid || !out) {
+    report("null argument");
+    return ICAM_ERR_ARG;
+  }
+  *out = nullptr;
+  IcamPack* pk = new IcamPack();
+  pk->device = opt ? opt->device : 0;
+  double need = opt && opt->need > 0 ? opt->need : 2.0;
+  std::string e;
+  if (!build_pack(solid, need, &pk->host, &e)) {
+    report(e);
+    delete pk;
+    return ICAM_ERR_PACK;
+  }
+  int rc = ICAM_OK;
+  auto cuda = [&](cudaError_t c, const char* what) {
+    if (c != cudaSuccess && rc == ICAM_OK) {
+      rc = ICAM_ERR_CUDA;
+      report(std::string(what) + ": " + cudaGetErrorString(c));
+    }
+  };
+  cuda(cudaSetDevice(pk->device), "cudaSetDevice");
+  if (rc == ICAM_OK) cuda(cudaStreamCreateWithFlags(&pk->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  if (rc != ICAM_OK) {
+    delete pk;
+    return rc;
+  }
+  HostPack& H = pk->host;
+  DPack& D = pk->dev;
+  int u = ICAM_OK;
+  u |= upload(pk, H.faces, &D.faces);
+  u |= upload(pk, H.nurbs, &D.nurbs);
+  u |= upload(pk, H.subs, &D.subs);
+  u |= upload(pk, H.sub_cp, &D.sub_cp);
+  u |= upload(pk, H.sub_cp32, &D.sub_cp32);
+  u |= upload(pk, H.span_cp, &D.span_cp);
+  u |= upload(pk, H.breaks, &D.breaks);
+  u |= upload(pk, H.edges, &D.edges);
+  u |= upload(pk, H.pieces, &D.pieces);
+  u |= upload(pk, H.verts, &D.verts);
+  u |= upload(pk, H.cells, &D.cells);
+  u |= upload(pk, H.insts, &D.insts);
+  u |= upload(pk, H.among, &D.among);
+  u |= upload(pk, H.tpieces, &D.tpieces);
+  u |= upload(pk, H.bvh, &D.bvh);
+  u |= upload(pk, H.items, &D.items);
+  for (int i = 0; i < int(H.bvh.size()); i++)
+    if (H.bvh[i].count > 0) pk->leaves_host.push_back(i);
+  const int32_t* lv = nullptr;
+  u |= upload(pk, pk->leaves_host, &lv);
+  pk->leaves = const_cast<int32_t*>(lv);
+  void* st = nullptr;
+  if (cudaMalloc(&st, 16 * sizeof(unsigned long long)) == cudaSuccess) {
+    pk->owned.push_back(st);
+    pk->d_stats = static_cast<unsigned long long*>(st);
+  } else {
+    u |= ICAM_ERR_CUDA;
+  }
+  if (u != ICAM_OK || cudaStreamSynchronize(pk->stream) != cudaSuccess) {
+    report("upload: " + pk->err);
+    icam_pack_destroy(pk);
+    return ICAM_ERR_CUDA;
+  }
+  D.n_faces = int(H.faces.size());
+  D.n_subs = int(H.subs.size());
+  D.n_edges = int(H.edges.size());
+  D.n_pieces = int(H.pieces.size());
+  D.n_verts = int(H.verts.size());
+  D.n_bvh = int(H.bvh.size());
+  D.n_items = int(H.items.size());
+  D.tol = H.tol;
+  for (int k = 0; k < 3; k++) D.lo[k] = H.lo[k], D.hi[k] = H.hi[k];
+  *out = pk;
+  return ICAM_OK;
+}
+
+void icam_pack_destroy(IcamPack* pk) {
+  if (!pk) return;
+  cudaSetDevice(pk->device);
+  if (pk->stream) cudaStreamSynchronize(pk->stream);
+  for (void* p : pk->owned) cudaFree(p);
+  for (auto& b : pk->scratch)
+    if (b.p) cudaFree(b.p);
+  if (pk->stream) cudaStreamDestroy(pk->stream);
+  delete pk;
+}
+
+int icam_pack_info(const IcamPack* pk, int64_t counts[7]) {
+  if (!pk || !counts) return ICAM_ERR_ARG;
+  counts[0] = pk->host.faces.size();
+  counts[1] = pk->host.edges.size();
+  counts[2] = pk->host.verts.size();
+  counts[3] = pk->host.subs.size();
+  counts[4] = pk->host.pieces.size();
+  counts[5] = pk->host.cells.size();
+  counts[6] = pk->host.bvh.size();
+  return ICAM_OK;
+}
+
+const char* icam_last_error(const IcamPack* pk) { return pk ? pk->err.c_str() : "null pack"; }
+
+int icam_points(IcamPack* pk, const double* xyz, size_t n, double clamp, int capped, int precision,
+                double* value_out, int8_t* flag_out) {
+  if (!pk || (!xyz && n) || (!value_out && n) || (!flag_out && n)) return fail(pk, ICAM_ERR_ARG, "null argument");
+  if (precision < ICAM_FP64 || precision > ICAM_MIXED_LEARNED) return fail(pk, ICAM_ERR_ARG, "unknown precision");
+  if (n == 0) return ICAM_OK;
+  CK(cudaSetDevice(pk->device));
+  void *dx, *dv, *df;
+  int r;
+  if ((r = scratch(pk, 0, n * 3 * sizeof(double), &dx)) || (r = scratch(pk, 1, n * sizeof(double), &dv)) ||
+      (r = scratch(pk, 2, n, &df)))
+    return r;
+  CK(cudaMemcpyAsync(dx, xyz, n * 3 * sizeof(double), cudaMemcpyHostToDevice, pk->stream));
+  double cap = capped ? clamp : INFINITY;
+  k_points<<<grid_for(int64_t(n), 128), 128, 0, pk->stream>>>(pk->dev, (const double*)dx, int64_t(n), cap,
+                                                               (double*)dv, (int8_t*)df);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(value_out, dv, n * sizeof(double), cudaMemcpyDeviceToHost, pk->stream));
+  CK(cudaMemcpyAsync(flag_out, df, n, cudaMemcpyDeviceToHost, pk->stream));
+  CK(cudaStreamSynchronize(pk->stream));
+  return ICAM_OK;
+}
+
+int icam_bricks(IcamPack* pk, const double* first_nodes, size_t n, double h, double clamp, int precision,
+                float* values_out, double* d_out) {
+  if (!pk || (!first_nodes && n)) return fail(pk, ICAM_ERR_ARG, "null argument");
+  if (!(h > 0) || !(clamp > 0)) return fail(pk, ICAM_ERR_ARG, "h and clamp must be positive");
+  if (precision < ICAM_FP64 || precision > ICAM_MIXED_LEARNED) return fail(pk, ICAM_ERR_ARG, "unknown precision");
+  if (n == 0) return ICAM_OK;
+  CK(cudaSetDevice(pk->device));
+  void *dfirst, *dval, *dflag;
+  int r;
+  if ((r = scratch(pk, 0, n * 3 * sizeof(double), &dfirst)) || (r = scratch(pk, 1, n * 729 * sizeof(double), &dval)) ||
+      (r = scratch(pk, 2, n * 729, &dflag)))
+    return r;
+  CK(cudaMemcpyAsync(dfirst, first_nodes, n * 3 * sizeof(double), cudaMemcpyHostToDevice, pk->stream));
+  BrickArgs a{};
+  a.P = pk->dev;
+  a.firsts = (const double*)dfirst;
+  a.dcs = nullptr;
+  a.n = int64_t(n);
+  a.h = h;
+  a.clamp = clamp;
+  a.leaves = pk->leaves;
+  a.n_leaves = int32_t(pk->leaves_host.size());
+  a.mixed = precision != ICAM_FP64;
+  a.d_out = (double*)dval;
+  a.flag_out = (int8_t*)dflag;
+  a.stats = pk->d_stats;
+  CK(cudaMemsetAsync(pk->d_stats, 0, 16 * sizeof(unsigned long long), pk->stream));
+  k_bricks<<<grid_for(int64_t(n), 1), 256, 0, pk->stream>>>(a);
+  CK(cudaGetLastError());
+  std::vector<double> v(n * 729);
+  std::vector<int8_t> f(n * 729);
+  CK(cudaMemcpyAsync(v.data(), dval, n * 729 * sizeof(double), cudaMemcpyDeviceToHost, pk->stream));
+  CK(cudaMemcpyAsync(f.data(), dflag, n * 729, cudaMemcpyDeviceToHost, pk->stream));
+  CK(cudaStreamSynchronize(pk->stream));
+  for (size_t i = 0; i < n * 729; i++) {
+    if (values_out) {
+      values_out[2 * i] = float(v[i]);
+      values_out[2 * i + 1] = float(f[i]);
+    }
+    if (d_out) d_out[i] = v[i];
+  }
+  return ICAM_OK;
+}
+
+// The level bake; results left in device scratch.
+static int bake_level(IcamPack* pk, double h, const double lo[3], const int64_t nb[3], double clamp,
+                      const double origin[3], int precision, size_t* n_slots, IcamBakeStats* stats,
+                      const uint32_t** d_map_out, const uint32_t** d_atlas_out) {
+  if (!pk || !lo || !nb || !n_slots) return fail(pk, ICAM_ERR_ARG, "null argument");
+  if (!(h > 0) || !(clamp > 0)) return fail(pk, ICAM_ERR_ARG, "h and clamp must be positive");
+  if (nb[0] <= 0 || nb[1] <= 0 || nb[2] <= 0) return fail(pk, ICAM_ERR_ARG, "nb must be positive");
+  if (precision < ICAM_FP64 || precision > ICAM_MIXED_LEARNED) return fail(pk, ICAM_ERR_ARG, "unknown precision");
+  CK(cudaSetDevice(pk->device));
+  cudaStream_t s = pk->stream;
+  int64_t total = nb[0] * nb[1] * nb[2];
+  if (total > (int64_t(1) << 34)) return fail(pk, ICAM_ERR_ARG, "level too large");
+  cudaEvent_t ev[5];
+  for (auto& e : ev) CK(cudaEventCreate(&e));
+  CK(cudaEventRecord(ev[0], s));
+  int64_t launches = 0;
+  void *d_map, *d_cur, *d_next, *d_ridx, *d_rdc, *d_cnt;
+  int r;
+  // box lists: at most 8x the boxes of the previous size; bounded by the level's bricks
+  int64_t box_cap = std::max<int64_t>(total + 64, 1 << 12);
+  if ((r = scratch(pk, 3, total * sizeof(uint32_t), &d_map)) || (r = scratch(pk, 4, box_cap * sizeof(Box4), &d_cur)) ||
+      (r = scratch(pk, 5, box_cap * sizeof(Box4), &d_next)) || (r = scratch(pk, 6, total * sizeof(int64_t), &d_ridx)) ||
+      (r = scratch(pk, 7, total * sizeof(double), &d_rdc)) || (r = scratch(pk, 8, 4 * sizeof(unsigned long long), &d_cnt)))
+    return r;
+  CK(cudaMemsetAsync(d_cnt, 0, 4 * sizeof(unsigned long long), s));
+  // the first boxes, on the grid aligned on the origin (partcache.rs:250-270)
+  long long nbmax = std::max(nb[0], std::max(nb[1], nb[2]));
+  long long size = 1;
+  while (size < nbmax) size *= 2;
+  double side = 8.0 * h;
+  double o[3] = {origin ? origin[0] - h : lo[0] - 0.0, origin ? origin[1] - h : lo[1], origin ? origin[2] - h : lo[2]};
+  long long g0[3], start[3];
+  for (int k = 0; k < 3; k++) {
+    g0[k] = origin ? (long long)std::llround((lo[k] - o[k]) / side) : 0;
+    long long q = g0[k] >= 0 ? g0[k] / size : -((-g0[k] + size - 1) / size);
+    start[k] = q * size - g0[k];
+  }
+  std::vector<Box4> first;
+  for (long long z = start[2]; z < nb[2]; z += size)
+    for (long long y = start[1]; y < nb[1]; y += size)
+      for (long long x = start[0]; x < nb[0]; x += size) first.push_back({x, y, z, NAN, INFINITY});
+  CK(cudaMemcpyAsync(d_cur, first.data(), first.size() * sizeof(Box4), cudaMemcpyHostToDevice, s));
+  int64_t ncur = int64_t(first.size()), boxes_read = 0;
+  unsigned long long* cnt = (unsigned long long*)d_cnt;
+  while (ncur > 0) {
+    DecideArgs a{};
+    a.P = pk->dev;
+    a.boxes = (const Box4*)d_cur;
+    a.n = ncur;
+    a.size = size;
+    a.h = h;
+    a.clamp = clamp;
+    for (int k = 0; k < 3; k++) a.lo[k] = lo[k], a.nb[k] = nb[k];
+    a.map = (uint32_t*)d_map;
+    a.next = (Box4*)d_next;
+    a.next_cap = box_cap;
+    a.n_next = cnt + 0;
+    a.read_idx = (int64_t*)d_ridx;
+    a.read_dc = (double*)d_rdc;
+    a.read_cap = total;
+    a.n_read = cnt + 1;
+    CK(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), s));
+    k_decide<<<grid_for(ncur, 64), 64, 0, s>>>(a);
+    launches++;
+    CK(cudaGetLastError());
+    unsigned long long nn = 0;
+    CK(cudaMemcpyAsync(&nn, cnt, sizeof(nn), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    boxes_read += ncur;
+    if (int64_t(nn) > box_cap) return fail(pk, ICAM_ERR_ROOM, "box list overflow");
+    std::swap(d_cur, d_next);
+    ncur = int64_t(nn);
+    size /= 2;
+  }
+  unsigned long long nread = 0;
+  CK(cudaMemcpyAsync(&nread, cnt + 1, sizeof(nread), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  CK(cudaEventRecord(ev[1], s));
+  int64_t R = int64_t(nread);
+  // the read bricks in brick order (partcache.rs:486)
+  void *d_ridx2, *d_rdc2, *d_tmp, *d_first, *d_words, *d_kind, *d_flag, *d_slot, *d_atlas;
+  size_t tmp_bytes = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, (int64_t*)nullptr, (int64_t*)nullptr, (double*)nullptr,
+                                  (double*)nullptr, R, 0, 64, s);
+  size_t scan_bytes = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (int64_t*)nullptr, (int64_t*)nullptr, R + 1, s);
+  tmp_bytes = std::max(tmp_bytes, scan_bytes);
+  size_t Rb = size_t(std::max<int64_t>(R, 1));
+  if ((r = scratch(pk, 9, Rb * sizeof(int64_t), &d_ridx2)) || (r = scratch(pk, 10, Rb * sizeof(double), &d_rdc2)) ||
+      (r = scratch(pk, 11, tmp_bytes + 16, &d_tmp)) || (r = scratch(pk, 12, Rb * 3 * sizeof(double), &d_first)) ||
+      (r = scratch(pk, 13, Rb * 365 * sizeof(uint32_t), &d_words)) || (r = scratch(pk, 14, Rb * sizeof(int32_t), &d_kind)) ||
+      (r = scratch(pk, 15, (Rb + 1) * 2 * sizeof(int64_t), &d_flag)))
+    return r;
+  d_slot = (int64_t*)d_flag + (Rb + 1);
+  size_t nwords_slots = 0;
+  if (R > 0) {
+    CK(cub::DeviceRadixSort::SortPairs(d_tmp, tmp_bytes, (const int64_t*)d_ridx, (int64_t*)d_ridx2,
+                                       (const double*)d_rdc, (double*)d_rdc2, R, 0, 64, s));
+    k_gather_firsts<<<grid_for(R, 256), 256, 0, s>>>((const int64_t*)d_ridx2, R, nb[0], nb[1], h, lo[0], lo[1], lo[2],
+                                                    (double*)d_first);
+    launches += 2;
+    CK(cudaEventRecord(ev[2], s));
+    BrickArgs b{};
+    b.P = pk->dev;
+    b.firsts = (const double*)d_first;
+    b.dcs = (const double*)d_rdc2;
+    b.n = R;
+    b.h = h;
+    b.clamp = clamp;
+    b.leaves = pk->leaves;
+    b.n_leaves = int32_t(pk->leaves_host.size());
+    b.mixed = precision != ICAM_FP64;
+    b.words_out = (uint32_t*)d_words;
+    b.kind_out = (int32_t*)d_kind;
+    b.stats = pk->d_stats;
+    CK(cudaMemsetAsync(pk->d_stats, 0, 16 * sizeof(unsigned long long), s));
+    k_bricks<<<grid_for(R, 1), 256, 0, s>>>(b);
+    launches++;
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ev[3], s));
+    // slots: stored bricks numbered in brick order
+    k_is_words<<<grid_for(R, 256), 256, 0, s>>>((const int32_t*)d_kind, R, (int64_t*)d_flag);
+    CK(cudaMemsetAsync((int64_t*)d_flag + R, 0, sizeof(int64_t), s));
+    CK(cub::DeviceScan::ExclusiveSum(d_tmp, tmp_bytes, (const int64_t*)d_flag, (int64_t*)d_slot, R + 1, s));
+    int64_t ns = 0;
+    CK(cudaMemcpyAsync(&ns, (int64_t*)d_slot + R, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    nwords_slots = size_t(ns);
+    if ((r = scratch(pk, 2, std::max<size_t>(nwords_slots, 1) * 365 * sizeof(uint32_t), &d_atlas))) return r;
+    k_assemble<<<grid_for(R, 1), 128, 0, s>>>((const int64_t*)d_ridx2, (const int32_t*)d_kind, (const int64_t*)d_slot,
+                                              R, (const uint32_t*)d_words, (uint32_t*)d_map, (uint32_t*)d_atlas);
+    launches += 3;
+    CK(cudaGetLastError());
+  } else {
+    CK(cudaEventRecord(ev[2], s));
+    CK(cudaEventRecord(ev[3], s));
+    if ((r = scratch(pk, 2, 365 * sizeof(uint32_t), &d_atlas))) return r;
+  }
+  CK(cudaEventRecord(ev[4], s));
+  CK(cudaStreamSynchronize(s));
+  *n_slots = nwords_slots;
+  *d_map_out = (const uint32_t*)d_map;
+  *d_atlas_out = (const uint32_t*)d_atlas;
+  if (stats) {
+    unsigned long long st[16] = {0};
+    CK(cudaMemcpy(st, pk->d_stats, sizeof(st), cudaMemcpyDeviceToHost));
+    std::memset(stats, 0, sizeof(*stats));
+    stats->boxes_read = boxes_read;
+    stats->bricks_read = R;
+    stats->bricks_words = int64_t(nwords_slots);
+    stats->nodes_exact = R ? int64_t(st[0]) : 0;
+    stats->nodes_far = R ? int64_t(st[1]) : 0;
+    stats->nodes_undecided = R ? int64_t(st[2]) : 0;
+    stats->pairs = R ? int64_t(st[4]) : 0;
+    stats->kernel_launches = launches;
+    float ms;
+    cudaEventElapsedTime(&ms, ev[0], ev[1]);
+    stats->ms_decide = ms;
+    cudaEventElapsedTime(&ms, ev[2], ev[3]);
+    stats->ms_nodes = ms;
+    cudaEventElapsedTime(&ms, ev[3], ev[4]);
+    stats->ms_post = ms;
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  return ICAM_OK;
+}
+
+int icam_bake_level(IcamPack* pk, double h, const double lo[3], const int64_t nb[3], double clamp,
+                    const double origin[3], int precision, uint32_t* map_out, uint32_t* atlas_out,
+                    size_t atlas_cap_words, size_t* n_slots, IcamBakeStats* stats) {
+  const uint32_t *dm, *da;
+  int rc = bake_level(pk, h, lo, nb, clamp, origin, precision, n_slots, stats, &dm, &da);
+  if (rc) return rc;
+  int64_t total = nb[0] * nb[1] * nb[2];
+  if (map_out) CK(cudaMemcpyAsync(map_out, dm, total * sizeof(uint32_t), cudaMemcpyDeviceToHost, pk->stream));
+  if (atlas_out) {
+    if (*n_slots * 365 > atlas_cap_words) return fail(pk, ICAM_ERR_ARG, "atlas_out too small");
+    CK(cudaMemcpyAsync(atlas_out, da, *n_slots * 365 * sizeof(uint32_t), cudaMemcpyDeviceToHost, pk->stream));
+  }
+  CK(cudaStreamSynchronize(pk->stream));
+  return ICAM_OK;
+}
+
+int icam_bake_level_device(IcamPack* pk, double h, const double lo[3], const int64_t nb[3], double clamp,
+                           const double origin[3], int precision, const uint32_t** d_map, const uint32_t** d_atlas,
+                           size_t* n_slots, IcamBakeStats* stats) {
+  if (!d_map || !d_atlas) return fail(pk, ICAM_ERR_ARG, "null argument");
+  return bake_level(pk, h, lo, nb, clamp, origin, precision, n_slots, stats, d_map, d_atlas);
+}
+
+int icam_list(const IcamPack* pk, const double c[3], double r, double d, uint32_t* codes, size_t cap, size_t* n) {
+  if (!pk || !c || !n) return ICAM_ERR_ARG;
+  const HostPack& H = pk->host;
+  double reach = d + 2.0 * r;
+  V cc(c[0], c[1], c[2]);
+  size_t k = 0;
+  std::vector<int> stack = {0};
+  while (!stack.empty()) {
+    const DBvh& nd = H.bvh[stack.back()];
+    stack.pop_back();
+    Bx b;
+    b.add(V(nd.lo[0], nd.lo[1], nd.lo[2]));
+    b.add(V(nd.hi[0], nd.hi[1], nd.hi[2]));
+    if (b.dist(cc) > reach) continue;
+    if (nd.count == 0) {
+      stack.push_back(nd.first);
+      stack.push_back(nd.first + 1);
+      continue;
+    }
+    for (int i = 0; i < nd.count; i++) {
+      uint32_t code = H.items[nd.first + i];
+      uint32_t kind = code >> IK_SHIFT, idx = code & IK_MASK;
+      const double* box = kind == IK_FACE ? H.faces[idx].box
+                          : kind == IK_SUB ? H.subs[idx].box
+                          : kind == IK_EDGE ? H.edges[idx].box
+                          : kind == IK_PIECE ? H.pieces[idx].box
+                                             : nullptr;
+      double lb;
+      if (box) {
+        Bx ib;
+        ib.add(V(box[0], box[1], box[2]));
+        ib.add(V(box[3], box[4], box[5]));
+        lb = ib.dist(cc);
+      } else {
+        lb = (cc - V(H.verts[idx].p[0], H.verts[idx].p[1], H.verts[idx].p[2])).len();
+      }
+      if (lb <= reach) {
+        if (k < cap && codes) codes[k] = code;
+        k++;
+      }
+    }
+  }
+  *n = k;
+  return ICAM_OK;
+}
+
+int icam_warm(IcamPack* pk, double secs) {
+  if (!pk) return ICAM_ERR_ARG;
+  CK(cudaSetDevice(pk->device));
+  void* d;
+  int r;
+  if ((r = scratch(pk, 0, 64, &d))) return r;
+  auto t0 = std::chrono::steady_clock::now();
+  while (std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() < secs) {
+    k_warm<<<1024, 256, 0, pk->stream>>>((float*)d, 4096);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(pk->stream));
+  }
+  return ICAM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,62 @@
+// Launch arguments of the field kernels (kernels.cu) and their declarations.
+#pragma once
+
+#include <cstdint>
+
+#include "pack.h"
+
+namespace icam {
+
+// A box of bricks being decided: its first brick, its parent's signed distance at the
+// parent's centre (NaN when not known) and how far that centre is from its own.
+struct Box4 {
+  long long x, y, z;
+  double parent_sd;
+  double reach;
+};
+
+struct BrickArgs {
+  DPack P;
+  const double* firsts;  // n x 3 first nodes
+  const double* dcs;     // n centre distances (NaN when not known), or null
+  int64_t n;
+  double h, clamp;
+  const int32_t* leaves;  // the tree's leaf nodes
+  int32_t n_leaves;
+  int32_t mixed;          // 1: single-precision bulk with double polish
+  double* d_out;          // optional n x 729 values
+  int8_t* flag_out;       // optional n x 729 flags
+  uint32_t* words_out;    // optional n x 365 packed words
+  int32_t* kind_out;      // optional n kinds (0 words, 1 air, 2 solid)
+  unsigned long long* stats;  // exact, far, undecided, bridged, pairs, overflows
+};
+
+struct DecideArgs {
+  DPack P;
+  const Box4* boxes;
+  int64_t n;
+  long long size;
+  double h, clamp;
+  double lo[3];
+  long long nb[3];
+  uint32_t* map;
+  Box4* next;
+  int64_t next_cap;
+  unsigned long long* n_next;
+  int64_t* read_idx;
+  double* read_dc;
+  int64_t read_cap;
+  unsigned long long* n_read;
+};
+
+__global__ void k_points(DPack P, const double* xyz, int64_t n, double cap, double* value, int8_t* flag);
+__global__ void k_bricks(BrickArgs a);
+__global__ void k_decide(DecideArgs a);
+__global__ void k_gather_firsts(const int64_t* idx, int64_t n, int64_t nb0, int64_t nb1, double h, double lo0,
+                                double lo1, double lo2, double* firsts);
+__global__ void k_assemble(const int64_t* idx, const int32_t* kind, const int64_t* slot, int64_t n,
+                           const uint32_t* words, uint32_t* map, uint32_t* atlas);
+__global__ void k_is_words(const int32_t* kind, int64_t n, int64_t* flag);
+__global__ void k_warm(float* out, int iters);
+
+}  // namespace icam

@@ -1,0 +1,526 @@
+// Builds the device layout of a solid (pack.h) from its description (icam_solid.h):
+// trim trees per face, B-spline spans raised to bicubic and split into sub-patches
+// that certify convexity for the pack's `need`, flat spline-edge pieces with their
+// bounds, angle-weighted vertex pseudo-normals, and one bounding-volume tree over
+// every feature. Host code; the arrays are uploaded by the caller.
+#include "pack_build.h"
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+
+namespace icam {
+
+namespace {
+
+const double PI = 3.14159265358979323846;
+
+V vec(const double* x) { return V(x[0], x[1], x[2]); }
+
+struct Axial {
+  double theta, rho, h;
+  V er;
+};
+Axial axial(const DFace& f, V p) {
+  V d = p - vec(f.o);
+  V x = vec(f.x), y = vec(f.y), z = vec(f.z);
+  double lx = d.dot(x), ly = d.dot(y), lz = d.dot(z);
+  double rho = std::sqrt(lx * lx + ly * ly);
+  double th = rho > 0 ? std::atan2(ly, lx) : 0.0;
+  return {th, rho, lz, x * std::cos(th) + y * std::sin(th)};
+}
+
+// Outward normal of an analytic face at a point on it (surface3.rs:132-148 times the sense).
+V analytic_normal(const DFace& f, V q) {
+  V n;
+  switch (f.kind) {
+    case S_PLANE: n = vec(f.z); break;
+    case S_CYLINDER: n = axial(f, q).er; break;
+    case S_CONE: n = axial(f, q).er * std::cos(f.b) - vec(f.z) * std::sin(f.b); break;
+    case S_SPHERE: n = (q - vec(f.o)).unit(); break;
+    default: n = (q - (vec(f.o) + axial(f, q).er * f.a)).unit(); break;
+  }
+  return n * f.sense;
+}
+
+// The nearest point of a B-spline face's spans to a point on (or very near) it: Newton
+// from each span's middle, kept in its span; returns (u, v) and the unit normal Su x Sv.
+struct SpanGrid {
+  std::vector<Bicubic> spans;
+  int nsu, nsv;
+};
+void nearest_on(const SpanGrid& g, V x, double* u, double* v, V* n, double* dist) {
+  double best = 1e300;
+  for (auto& sp : g.spans) {
+    double s = 0.5, t = 0.5;
+    for (int it = 0; it < 40; it++) {
+      V P, Ps, Pt, Pss, Pst, Ptt;
+      sp.eval(s, t, &P, &Ps, &Pt, &Pss, &Pst, &Ptt);
+      V r = P - x;
+      double g0 = Ps.dot(r), g1 = Pt.dot(r);
+      double a = Ps.dot(Ps) + Pss.dot(r), b = Ps.dot(Pt) + Pst.dot(r), c = Pt.dot(Pt) + Ptt.dot(r);
+      if (!(a > 0 && a * c - b * b > 0)) a = Ps.dot(Ps), b = Ps.dot(Pt), c = Pt.dot(Pt);
+      double det = a * c - b * b;
+      if (std::fabs(det) < 1e-300) break;
+      double ds = -(c * g0 - b * g1) / det, dt = -(a * g1 - b * g0) / det;
+      double ns = std::min(std::max(s + ds, 0.0), 1.0), nt = std::min(std::max(t + dt, 0.0), 1.0);
+      double moved = std::fabs(ns - s) + std::fabs(nt - t);
+      s = ns, t = nt;
+      if (moved < 1e-15) break;
+    }
+    V P, Ps, Pt;
+    sp.eval(s, t, &P, &Ps, &Pt, nullptr, nullptr, nullptr);
+    double d = (P - x).len();
+    if (d < best) {
+      best = d;
+      *u = sp.u0 + s * (sp.u1 - sp.u0);
+      *v = sp.v0 + t * (sp.v1 - sp.v0);
+      *n = Ps.cross(Pt).unit();
+    }
+  }
+  *dist = best;
+}
+
+struct Item {
+  uint32_t code;
+  Bx box;
+};
+
+// Median split on the longest axis of the centroids' box, into the node at `slot`;
+// leaves of at most 4, a node's two children stored side by side.
+void build_bvh(std::vector<Item>& items, int a, int b, int slot, std::vector<DBvh>& nodes,
+               std::vector<uint32_t>& out_items) {
+  Bx bx, cb;
+  for (int i = a; i < b; i++) {
+    bx.add(items[i].box);
+    cb.add(items[i].box.mid());
+  }
+  for (int k = 0; k < 3; k++) {
+    nodes[slot].lo[k] = std::nextafter(float(bx.lo[k]), -INFINITY);
+    nodes[slot].hi[k] = std::nextafter(float(bx.hi[k]), INFINITY);
+  }
+  if (b - a <= 4) {
+    nodes[slot].first = int(out_items.size());
+    nodes[slot].count = b - a;
+    for (int i = a; i < b; i++) out_items.push_back(items[i].code);
+    return;
+  }
+  V ext = cb.hi - cb.lo;
+  int ax = ext.x >= ext.y && ext.x >= ext.z ? 0 : (ext.y >= ext.z ? 1 : 2);
+  int m = (a + b) / 2;
+  std::nth_element(items.begin() + a, items.begin() + m, items.begin() + b,
+                   [&](const Item& p, const Item& q) { return p.box.mid()[ax] < q.box.mid()[ax]; });
+  int kids = int(nodes.size());
+  nodes.resize(kids + 2);
+  nodes[slot].first = kids;
+  nodes[slot].count = 0;
+  build_bvh(items, a, m, kids, nodes, out_items);
+  build_bvh(items, m, b, kids + 1, nodes, out_items);
+}
+
+}  // namespace
+
+bool build_pack(const IcamSolidDesc* d, double need, HostPack* hp, std::string* err) {
+  HostPack& P = *hp;
+  P = HostPack();
+  P.tol = d->tol;
+  if (d->n_faces <= 0 || d->n_edges <= 0 || d->n_verts <= 0) {
+    *err = "empty solid";
+    return false;
+  }
+  // ---------------------------------------------------------------- faces and spans
+  std::vector<SpanGrid> grids(d->n_faces);
+  std::vector<TrimTree> trees(d->n_faces);
+  for (int fi = 0; fi < d->n_faces; fi++) {
+    const IcamFaceDesc& fd = d->faces[fi];
+    DFace f{};
+    f.kind = fd.kind;
+    f.sense = fd.sense >= 0 ? 1.0 : -1.0;
+    for (int k = 0; k < 3; k++) {
+      f.o[k] = fd.f.o[k];
+      f.z[k] = fd.f.z[k];
+      f.x[k] = fd.f.x[k];
+    }
+    V y = vec(f.z).cross(vec(f.x));
+    f.y[0] = y.x, f.y[1] = y.y, f.y[2] = y.z;
+    f.a = fd.a;
+    f.b = fd.b;
+    for (int k = 0; k < 2; k++) {
+      f.lo[k] = fd.lo[k];
+      f.hi[k] = fd.hi[k];
+      f.period[k] = fd.period[k];
+    }
+    f.nurbs = -1;
+    if (fd.kind == ICAM_NURBS) {
+      if (fd.du < 1 || fd.du > 3 || fd.dv < 1 || fd.dv > 3) {
+        *err = "face " + std::to_string(fi) + ": B-spline degrees above 3 are not packed";
+        return false;
+      }
+      DNurbs nb{};
+      nb.face = fi;
+      nb.first_span = int(P.span_cp.size() / 16);
+      nb.nsu = fd.nsu;
+      nb.nsv = fd.nsv;
+      nb.first_break = int(P.breaks.size());
+      const double* br = d->breaks + fd.brk_off;
+      for (int k = 0; k <= fd.nsu + fd.nsv + 1; k++) P.breaks.push_back(br[k]);
+      int np = (fd.du + 1) * (fd.dv + 1);
+      grids[fi].nsu = fd.nsu;
+      grids[fi].nsv = fd.nsv;
+      for (int a = 0; a < fd.nsu; a++)
+        for (int b = 0; b < fd.nsv; b++) {
+          const double* c = d->patches + fd.patch_off + size_t(a * fd.nsv + b) * np * 4;
+          // rows along v raised to cubic, then columns along u
+          std::vector<std::vector<H>> rows(fd.du + 1);
+          for (int i = 0; i <= fd.du; i++) {
+            std::vector<H> r;
+            for (int j = 0; j <= fd.dv; j++) r.push_back({c[4 * (i * (fd.dv + 1) + j)], c[4 * (i * (fd.dv + 1) + j) + 1], c[4 * (i * (fd.dv + 1) + j) + 2], c[4 * (i * (fd.dv + 1) + j) + 3]});
+            while (r.size() < 4) r = elevate(r);
+            rows[i] = r;
+          }
+          Bicubic bc;
+          for (int j = 0; j < 4; j++) {
+            std::vector<H> col;
+            for (int i = 0; i <= fd.du; i++) col.push_back(rows[i][j]);
+            while (col.size() < 4) col = elevate(col);
+            for (int i = 0; i < 4; i++) bc.p[i][j] = col[i];
+          }
+          bc.u0 = br[a];
+          bc.u1 = br[a + 1];
+          bc.v0 = br[fd.nsu + 1 + b];
+          bc.v1 = br[fd.nsu + 1 + b + 1];
+          grids[fi].spans.push_back(bc);
+          for (int i = 0; i < 4; i++)
+            for (int j = 0; j < 4; j++) {
+              const H& h = bc.p[i][j];
+              P.span_cp.push_back({h[0], h[1], h[2], h[3]});
+            }
+        }
+      f.nurbs = int(P.nurbs.size());
+      P.nurbs.push_back(nb);
+    } else if (fd.kind < 0 || fd.kind > 4) {
+      *err = "face " + std::to_string(fi) + ": unknown surface kind";
+      return false;
+    }
+    // trim loops from the uses' parameter-domain curves (seams are not boundaries)
+    std::vector<TP> raw;
+    for (int k = 0; k < fd.n_uses; k++) {
+      const IcamUseDesc& u = d->uses[fd.first_use + k];
+      if (u.seam) continue;
+      for (int j = 0; j < u.n_pc; j++) {
+        TP t;
+        const double* c = d->pcurves + size_t(u.first_pc + j) * 12;
+        for (int i = 0; i < 4; i++)
+          for (int q = 0; q < 3; q++) t.c[i][q] = c[3 * i + q];
+        raw.push_back(t);
+      }
+    }
+    std::string e2;
+    if (!trees[fi].build(raw, fd.lo, fd.hi, fd.period, f.sense > 0, &e2)) {
+      *err = "face " + std::to_string(fi) + ": " + e2;
+      return false;
+    }
+    const TrimTree& tt = trees[fi];
+    if (tt.pieces.empty()) {
+      f.trim = -1;
+    } else {
+      int c0 = int(P.cells.size()), i0 = int(P.insts.size()), p0 = int(P.tpieces.size() / 12);
+      for (auto& pc : tt.pieces)
+        for (int i = 0; i < 4; i++)
+          for (int q = 0; q < 3; q++) P.tpieces.push_back(pc.c[i][q]);
+      for (auto& in : tt.inst) P.insts.push_back({p0 + in.first, 0, {in.second[0], in.second[1]}});
+      for (auto& c : tt.cells) {
+        DCell dc{};
+        for (int k = 0; k < 2; k++) {
+          dc.lo[k] = c.lo[k];
+          dc.hi[k] = c.hi[k];
+          dc.r[k] = c.r[k];
+        }
+        dc.inside = c.inside;
+        dc.kind = c.kind;
+        if (c.kind == 1) {
+          dc.first = int(P.among.size());
+          dc.count = int(c.among.size());
+          for (int i : c.among) P.among.push_back(i0 + i);
+        }
+        if (c.kind == 2)
+          for (int k = 0; k < 4; k++) dc.kids[k] = c0 + c.kids[k];
+        P.cells.push_back(dc);
+      }
+      f.trim = c0;
+    }
+    P.faces.push_back(f);
+  }
+  // ---------------------------------------------------------------- edges
+  for (int ei = 0; ei < d->n_edges; ei++) {
+    const IcamEdgeDesc& ed = d->edges[ei];
+    DEdge e{};
+    e.kind = ed.kind;
+    e.f0 = ed.f0;
+    e.f1 = ed.f1;
+    Bx box;
+    if (ed.kind == ICAM_EDGE_LINE) {
+      for (int k = 0; k < 3; k++) e.a[k] = ed.a[k], e.b[k] = ed.b[k];
+      box.add(vec(e.a));
+      box.add(vec(e.b));
+    } else if (ed.kind == ICAM_EDGE_ARC) {
+      for (int k = 0; k < 3; k++) e.o[k] = ed.f.o[k], e.z[k] = ed.f.z[k], e.x[k] = ed.f.x[k];
+      V y = vec(e.z).cross(vec(e.x));
+      e.y[0] = y.x, e.y[1] = y.y, e.y[2] = y.z;
+      e.r = ed.r;
+      e.t0 = ed.t0;
+      e.sweep = ed.sweep;
+      // the whole circle's box (curve3.rs:690-696)
+      V axes[3] = {V(1, 0, 0), V(0, 1, 0), V(0, 0, 1)};
+      for (V ax : axes) {
+        double ex = std::sqrt(std::max(1.0 - std::pow(vec(e.z).dot(ax), 2), 0.0)) * e.r;
+        box.add(vec(e.o) + ax * ex);
+        box.add(vec(e.o) - ax * ex);
+      }
+    } else if (ed.kind == ICAM_EDGE_SPLINE) {
+      if (ed.degree < 1 || ed.degree > 3) {
+        *err = "edge " + std::to_string(ei) + ": spline degrees above 3 are not packed";
+        return false;
+      }
+      // flat pieces (curve3.rs:1017-1031: split until the control polygon turns <= 0.35)
+      std::vector<Cubic3> flat, stack;
+      for (int k = ed.n_pieces - 1; k >= 0; k--) {
+        const double* c = d->cpieces + size_t(ed.first_piece + k) * (ed.degree + 1) * 4;
+        std::vector<H> q;
+        for (int j = 0; j <= ed.degree; j++) q.push_back({c[4 * j], c[4 * j + 1], c[4 * j + 2], c[4 * j + 3]});
+        while (q.size() < 4) q = elevate(q);
+        Cubic3 z;
+        for (int j = 0; j < 4; j++) z.c[j] = q[j];
+        stack.push_back(z);
+      }
+      while (!stack.empty()) {
+        Cubic3 z = stack.back();
+        stack.pop_back();
+        if (z.turning() <= 0.35 || flat.size() > 100000) {
+          flat.push_back(z);
+        } else {
+          Cubic3 l, r;
+          z.split(0.5, &l, &r);
+          stack.push_back(r);
+          stack.push_back(l);
+        }
+      }
+      e.first_piece = int(P.pieces.size());
+      e.n_pieces = int(flat.size());
+      for (size_t k = 0; k < flat.size(); k++) {
+        DPiece pc{};
+        pc.edge = ei;
+        pc.first = k == 0;
+        pc.last = k + 1 == flat.size();
+        for (int j = 0; j < 4; j++)
+          for (int c = 0; c < 4; c++) pc.cp[j][c] = flat[k].c[j][c];
+        Bx pb = flat[k].box();
+        for (int c = 0; c < 3; c++) pc.box[c] = pb.lo[c], pc.box[3 + c] = pb.hi[c];
+        box.add(pb);
+        pc.thick = flat[k].thickness();
+        if (!piece_bounds(flat[k].c, &pc.lam, pc.d2)) {
+          *err = "edge " + std::to_string(ei) + ": a weight is not positive";
+          return false;
+        }
+        for (int side = 0; side < 2; side++) {
+          int fi = side == 0 ? ed.f0 : ed.f1;
+          for (int end = 0; end < 2; end++) pc.uv[side][end][0] = pc.uv[side][end][1] = -1e300;
+          if (fi < 0 || d->faces[fi].kind != ICAM_NURBS) continue;
+          for (int end = 0; end < 2; end++) {
+            double u, v, dist;
+            V n;
+            nearest_on(grids[fi], hv(flat[k].c[end * 3]), &u, &v, &n, &dist);
+            pc.uv[side][end][0] = u;
+            pc.uv[side][end][1] = v;
+          }
+        }
+        P.pieces.push_back(pc);
+      }
+    } else {
+      *err = "edge " + std::to_string(ei) + ": unknown curve kind";
+      return false;
+    }
+    if (ed.kind != ICAM_EDGE_SPLINE)
+      for (int side = 0; side < 2; side++) {
+        int fi = side == 0 ? ed.f0 : ed.f1;
+        if (fi >= 0 && d->faces[fi].kind == ICAM_NURBS) {
+          *err = "edge " + std::to_string(ei) + ": a line or arc edge of a B-spline face is not packed";
+          return false;
+        }
+      }
+    for (int c = 0; c < 3; c++) e.box[c] = box.lo[c], e.box[3 + c] = box.hi[c];
+    P.edges.push_back(e);
+  }
+  // ---------------------------------------------------------------- face boxes (solid3.rs:1211-1278)
+  for (int fi = 0; fi < d->n_faces; fi++) {
+    DFace& f = P.faces[fi];
+    const IcamFaceDesc& fd = d->faces[fi];
+    Bx bx;
+    auto circle_box = [&](V c, V z, double r) {
+      V axes[3] = {V(1, 0, 0), V(0, 1, 0), V(0, 0, 1)};
+      for (V ax : axes) {
+        double e = std::sqrt(std::max(1.0 - std::pow(z.dot(ax), 2), 0.0)) * r;
+        bx.add(c + ax * e);
+        bx.add(c - ax * e);
+      }
+    };
+    auto edge_box = [&](int ei) {
+      Bx b;
+      b.add(V(P.edges[ei].box[0], P.edges[ei].box[1], P.edges[ei].box[2]));
+      b.add(V(P.edges[ei].box[3], P.edges[ei].box[4], P.edges[ei].box[5]));
+      return b;
+    };
+    if (f.kind == S_PLANE) {
+      for (int k = 0; k < fd.n_uses; k++) bx.add(edge_box(d->uses[fd.first_use + k].edge));
+    } else if (f.kind == S_CYLINDER || f.kind == S_CONE) {
+      double h0 = 1e300, h1 = -1e300;
+      for (int k = 0; k < fd.n_uses; k++) {
+        Bx eb = edge_box(d->uses[fd.first_use + k].edge);
+        for (int q = 0; q < 8; q++) {
+          V c((q & 1) ? eb.hi.x : eb.lo.x, (q & 2) ? eb.hi.y : eb.lo.y, (q & 4) ? eb.hi.z : eb.lo.z);
+          double h = (c - vec(f.o)).dot(vec(f.z));
+          h0 = std::min(h0, h);
+          h1 = std::max(h1, h);
+        }
+      }
+      for (double h : {h0, h1}) circle_box(vec(f.o) + vec(f.z) * h, vec(f.z), f.kind == S_CONE ? std::fabs(f.a + h * std::tan(f.b)) : f.a);
+    } else if (f.kind == S_SPHERE) {
+      bx.add(vec(f.o) - V(f.a, f.a, f.a));
+      bx.add(vec(f.o) + V(f.a, f.a, f.a));
+    } else if (f.kind == S_TORUS) {
+      for (double h : {-f.b, f.b}) circle_box(vec(f.o) + vec(f.z) * h, vec(f.z), f.a + f.b);
+    } else {
+      for (auto& sp : grids[fi].spans) bx.add(sp.box());
+    }
+    for (int c = 0; c < 3; c++) f.box[c] = bx.lo[c], f.box[3 + c] = bx.hi[c];
+  }
+  // ---------------------------------------------------------------- sub-patches
+  for (int fi = 0; fi < d->n_faces; fi++) {
+    if (P.faces[fi].nurbs < 0) continue;
+    const SpanGrid& g = grids[fi];
+    for (int a = 0; a < g.nsu; a++)
+      for (int b = 0; b < g.nsv; b++) {
+        std::vector<std::pair<Bicubic, int>> todo = {{g.spans[a * g.nsv + b], 0}};
+        while (!todo.empty()) {
+          Bicubic sp = todo.back().first;
+          int depth = todo.back().second;
+          todo.pop_back();
+          DSub s{};
+          double rho;
+          if (!patch_bounds(sp, &s.sa, &s.sb, &s.lam, s.d2, &rho)) {
+            *err = "face " + std::to_string(fi) + ": a weight is not positive";
+            return false;
+          }
+          Bx bx = sp.box();
+          s.diag = (bx.hi - bx.lo).len();
+          if (rho < need + s.diag && depth < 3) {
+            Bicubic l, r, ll, lr, rl, rr;
+            sp.split_u(0.5, &l, &r);
+            l.split_v(0.5, &ll, &lr);
+            r.split_v(0.5, &rl, &rr);
+            for (Bicubic* q : {&rr, &rl, &lr, &ll}) todo.push_back({*q, depth + 1});
+            continue;
+          }
+          double plo[2] = {sp.u0, sp.v0}, phi[2] = {sp.u1, sp.v1};
+          int klass = trees[fi].box_class(plo, phi);
+          if (klass == 0) continue;  // wholly outside its face
+          s.face = fi;
+          s.nurbs = P.faces[fi].nurbs;
+          s.span_a = a;
+          s.span_b = b;
+          s.klass = klass;
+          s.u0 = sp.u0, s.u1 = sp.u1, s.v0 = sp.v0, s.v1 = sp.v1;
+          for (int c = 0; c < 3; c++) s.box[c] = bx.lo[c], s.box[3 + c] = bx.hi[c];
+          V mid = bx.mid();
+          s.c[0] = mid.x, s.c[1] = mid.y, s.c[2] = mid.z;
+          P.subs.push_back(s);
+          for (int i = 0; i < 4; i++)
+            for (int j = 0; j < 4; j++) {
+              const H& h = sp.p[i][j];
+              P.sub_cp.push_back({h[0], h[1], h[2], h[3]});
+              P.sub_cp32.push_back({float(h[0] - mid.x * h[3]), float(h[1] - mid.y * h[3]), float(h[2] - mid.z * h[3]), float(h[3])});
+            }
+        }
+      }
+  }
+  // ---------------------------------------------------------------- vertices (solid3.rs:797-834)
+  std::vector<V> pn(d->n_verts);
+  auto tangent_at = [&](int ei, double s) {
+    const DEdge& e = P.edges[ei];
+    if (e.kind == 0) return (vec(e.b) - vec(e.a)).unit();
+    if (e.kind == 1) {
+      double t = e.t0 + s * e.sweep;
+      return (vec(e.x) * (-std::sin(t)) + vec(e.y) * std::cos(t)) * (e.sweep >= 0 ? 1.0 : -1.0);
+    }
+    int n = e.n_pieces;
+    int k = std::min(int(s * n), n - 1);
+    Cubic3 z;
+    for (int j = 0; j < 4; j++)
+      for (int c = 0; c < 4; c++) z.c[j][c] = P.pieces[e.first_piece + k].cp[j][c];
+    V p, d1;
+    z.eval(s * n - k, &p, &d1);
+    return d1.unit();
+  };
+  auto face_normal = [&](int fi, V x) {
+    const DFace& f = P.faces[fi];
+    if (f.kind != S_NURBS) return analytic_normal(f, x);
+    double u, v, dist;
+    V n;
+    nearest_on(grids[fi], x, &u, &v, &n, &dist);
+    return n * f.sense;
+  };
+  for (int fi = 0; fi < d->n_faces; fi++) {
+    const IcamFaceDesc& fd = d->faces[fi];
+    int k = 0;
+    while (k < fd.n_uses) {
+      int loop = d->uses[fd.first_use + k].loop, e0 = k;
+      while (k < fd.n_uses && d->uses[fd.first_use + k].loop == loop) k++;
+      int len = k - e0;
+      for (int i = 0; i < len; i++) {
+        const IcamUseDesc& ua = d->uses[fd.first_use + e0 + i];
+        const IcamUseDesc& ub = d->uses[fd.first_use + e0 + (i + 1) % len];
+        int vtx = ua.rev ? d->edges[ua.edge].v0 : d->edges[ua.edge].v1;
+        V x(d->verts[3 * vtx], d->verts[3 * vtx + 1], d->verts[3 * vtx + 2]);
+        V n = face_normal(fi, x);
+        auto use_tan = [&](const IcamUseDesc& u, double s) { return u.rev ? -tangent_at(u.edge, 1.0 - s) : tangent_at(u.edge, s); };
+        auto proj = [&](V t) { return (t - n * n.dot(t)).unit(); };
+        V ti = proj(use_tan(ua, 1.0)), to = proj(use_tan(ub, 0.0));
+        double turn = std::atan2(n.dot(ti.cross(to)), ti.dot(to));
+        pn[vtx] = pn[vtx] + n * (PI - turn);
+      }
+    }
+  }
+  for (int i = 0; i < d->n_verts; i++) {
+    DVert v{};
+    for (int k = 0; k < 3; k++) v.p[k] = d->verts[3 * i + k];
+    v.pn[0] = pn[i].x, v.pn[1] = pn[i].y, v.pn[2] = pn[i].z;
+    P.verts.push_back(v);
+  }
+  // ---------------------------------------------------------------- the tree over every feature
+  std::vector<Item> items;
+  Bx all;
+  auto box6 = [](const double* b) {
+    Bx x;
+    x.add(V(b[0], b[1], b[2]));
+    x.add(V(b[3], b[4], b[5]));
+    return x;
+  };
+  for (int i = 0; i < int(P.faces.size()); i++)
+    if (P.faces[i].kind != S_NURBS) items.push_back({(uint32_t(IK_FACE) << IK_SHIFT) | uint32_t(i), box6(P.faces[i].box)});
+  for (int i = 0; i < int(P.subs.size()); i++) items.push_back({(uint32_t(IK_SUB) << IK_SHIFT) | uint32_t(i), box6(P.subs[i].box)});
+  for (int i = 0; i < int(P.edges.size()); i++)
+    if (P.edges[i].kind != 2) items.push_back({(uint32_t(IK_EDGE) << IK_SHIFT) | uint32_t(i), box6(P.edges[i].box)});
+  for (int i = 0; i < int(P.pieces.size()); i++) items.push_back({(uint32_t(IK_PIECE) << IK_SHIFT) | uint32_t(i), box6(P.pieces[i].box)});
+  for (int i = 0; i < int(P.verts.size()); i++) {
+    Bx b;
+    b.add(V(P.verts[i].p[0], P.verts[i].p[1], P.verts[i].p[2]));
+    items.push_back({(uint32_t(IK_VERT) << IK_SHIFT) | uint32_t(i), b});
+  }
+  for (auto& it : items) all.add(it.box);
+  for (int k = 0; k < 3; k++) P.lo[k] = all.lo[k], P.hi[k] = all.hi[k];
+  P.bvh.assign(1, DBvh{});
+  build_bvh(items, 0, int(items.size()), 0, P.bvh, P.items);
+  return true;
+}
+
+}  // namespace icam

@@ -1,0 +1,184 @@
+"""Python binding of the C ABI (include/icam_cuda.h), mirroring the reference's GPU
+host for the part field, ``PartGpu`` (crates/icam-sim/src/partgpu.rs), and the level
+bake of ``PartCache`` (crates/icam-sim/src/partcache.rs).
+
+Every call runs the CUDA library ``libicam_cuda.so`` built in this package; there is
+no CPU path. A missing library or GPU raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .solid import IcamSolidDesc
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "libicam_cuda.so")
+
+FP64, MIXED, MIXED_LEARNED = 0, 1, 2
+AIR, SOLID, WORDS = 0xFFFFFFFF, 0xFFFFFFFE, 365
+
+_lib = None
+
+
+class IcamPackOptions(C.Structure):
+    _fields_ = [("device", C.c_int), ("need", C.c_double)]
+
+
+class IcamBakeStats(C.Structure):
+    _fields_ = [
+        ("boxes_read", C.c_int64), ("bricks_read", C.c_int64), ("bricks_words", C.c_int64),
+        ("nodes_exact", C.c_int64), ("nodes_far", C.c_int64), ("nodes_undecided", C.c_int64),
+        ("pairs", C.c_int64), ("fallback_nodes", C.c_int64), ("kernel_launches", C.c_int64),
+        ("ms_decide", C.c_double), ("ms_cull", C.c_double), ("ms_nodes", C.c_double), ("ms_post", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+def lib():
+    """The CUDA library, loaded once (raises when it is missing: build it with
+    ``python -m implicitcam_b200.build``)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            raise RuntimeError(f"{LIB} is missing: build it with `python -m implicitcam_b200.build`")
+        L = C.CDLL(LIB)
+        vp, sz = C.c_void_p, C.c_size_t
+        L.icam_pack_create.restype = C.c_int
+        L.icam_pack_create.argtypes = [vp, vp, C.POINTER(vp), C.c_char_p, sz]
+        L.icam_pack_destroy.argtypes = [vp]
+        L.icam_pack_info.argtypes = [vp, vp]
+        L.icam_last_error.restype = C.c_char_p
+        L.icam_last_error.argtypes = [vp]
+        L.icam_points.argtypes = [vp, vp, sz, C.c_double, C.c_int, C.c_int, vp, vp]
+        L.icam_bricks.argtypes = [vp, vp, sz, C.c_double, C.c_double, C.c_int, vp, vp]
+        L.icam_bake_level.argtypes = [vp, C.c_double, vp, vp, C.c_double, vp, C.c_int, vp, vp, sz, C.POINTER(sz), vp]
+        L.icam_bake_level_device.argtypes = [vp, C.c_double, vp, vp, C.c_double, vp, C.c_int, C.POINTER(vp),
+                                             C.POINTER(vp), C.POINTER(sz), vp]
+        L.icam_list.argtypes = [vp, vp, C.c_double, C.c_double, vp, sz, C.POINTER(sz)]
+        L.icam_warm.argtypes = [vp, C.c_double]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class IcamError(RuntimeError):
+    pass
+
+
+class PartGpu:
+    """The part packed on one GPU (PartGpu::new, partgpu.rs:132)."""
+
+    def __init__(self, solid, need: float = 2.0, device: int = 0):
+        desc = solid.desc() if hasattr(solid, "desc") else solid
+        assert isinstance(desc, IcamSolidDesc)
+        self._solid = solid
+        self._desc = desc
+        opt = IcamPackOptions(device, need)
+        h = C.c_void_p()
+        err = C.create_string_buffer(1024)
+        rc = lib().icam_pack_create(C.byref(desc), C.byref(opt), C.byref(h), err, 1024)
+        if rc != 0:
+            raise IcamError(f"icam_pack_create: {rc}: {err.value.decode()}")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().icam_pack_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise IcamError(f"{what}: {rc}: {lib().icam_last_error(self.h).decode()}")
+
+    def info(self):
+        c = np.zeros(7, np.int64)
+        lib().icam_pack_info(self.h, _p(c))
+        return dict(zip(["faces", "edges", "verts", "subs", "pieces", "cells", "bvh"], c.tolist()))
+
+    def points(self, xyz, clamp=np.inf, capped=False, precision=FP64):
+        """Signed distance of points: (value, flag) with flag 0 exact, 1 a bound past
+        the clamp, 2 undecided (PartGpu::points_scatter(_capped), partgpu.rs:243-264)."""
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        n = len(xyz)
+        v = np.zeros(n)
+        f = np.zeros(n, np.int8)
+        self._check(lib().icam_points(self.h, _p(xyz), n, float(clamp), int(capped), precision, _p(v), _p(f)),
+                    "icam_points")
+        return v, f
+
+    def bricks(self, firsts, h, clamp, precision=FP64):
+        """Every node of each brick (PartGpu::bricks, partgpu.rs:227): float pairs
+        (value, flag) as the reference returns them, and the double values."""
+        firsts = np.ascontiguousarray(firsts, dtype=np.float64).reshape(-1, 3)
+        n = len(firsts)
+        vals = np.zeros((n, 729, 2), np.float32)
+        d = np.zeros((n, 729))
+        self._check(lib().icam_bricks(self.h, _p(firsts), n, float(h), float(clamp), precision, _p(vals), _p(d)),
+                    "icam_bricks")
+        return vals, d
+
+    def level(self, h, lo, nb, clamp=None, origin=None, precision=FP64, atlas=True):
+        """One level of the brick cache (PartCache::level, partcache.rs:433):
+        (map, atlas (slots x 365 words), stats)."""
+        lo = np.ascontiguousarray(lo, dtype=np.float64)
+        nb = np.ascontiguousarray(nb, dtype=np.int64)
+        clamp = h * np.sqrt(3.0) if clamp is None else clamp
+        org = None if origin is None else np.ascontiguousarray(origin, dtype=np.float64)
+        m = np.zeros(int(np.prod(nb)), np.uint32)
+        ns = C.c_size_t()
+        st = IcamBakeStats()
+        # first the slot count, then the atlas sized to it
+        self._check(lib().icam_bake_level(self.h, float(h), _p(lo), _p(nb), float(clamp), _p(org), precision, _p(m),
+                                          None, 0, C.byref(ns), C.byref(st)), "icam_bake_level")
+        if not atlas:
+            return m, None, st.as_dict()
+        a = np.zeros((ns.value, WORDS), np.uint32)
+        self._check(lib().icam_bake_level(self.h, float(h), _p(lo), _p(nb), float(clamp), _p(org), precision, _p(m),
+                                          _p(a), a.size, C.byref(ns), C.byref(st)), "icam_bake_level")
+        return m, a, st.as_dict()
+
+    def level_device(self, h, lo, nb, clamp=None, origin=None, precision=FP64):
+        """The same bake with its results left on the device: (map ptr, atlas ptr, slots, stats)."""
+        lo = np.ascontiguousarray(lo, dtype=np.float64)
+        nb = np.ascontiguousarray(nb, dtype=np.int64)
+        clamp = h * np.sqrt(3.0) if clamp is None else clamp
+        org = None if origin is None else np.ascontiguousarray(origin, dtype=np.float64)
+        dm, da, ns = C.c_void_p(), C.c_void_p(), C.c_size_t()
+        st = IcamBakeStats()
+        self._check(lib().icam_bake_level_device(self.h, float(h), _p(lo), _p(nb), float(clamp), _p(org), precision,
+                                                 C.byref(dm), C.byref(da), C.byref(ns), C.byref(st)),
+                    "icam_bake_level_device")
+        return dm.value, da.value, ns.value, st.as_dict()
+
+    def list(self, c, r, d):
+        """Candidate codes (kind << 28 | index) within reach (PartGpu::list, partgpu.rs:220)."""
+        c = np.ascontiguousarray(c, dtype=np.float64)
+        out = np.zeros(1 << 16, np.uint32)
+        n = C.c_size_t()
+        self._check(lib().icam_list(self.h, _p(c), float(r), float(d), _p(out), out.size, C.byref(n)), "icam_list")
+        return out[: min(n.value, out.size)].copy()
+
+    def warm(self, secs):
+        self._check(lib().icam_warm(self.h, float(secs)), "icam_warm")
+
+
+def unpack_atlas(atlas):
+    """The i16 node values of each slot (729 a brick, x fastest)."""
+    a = np.asarray(atlas, dtype=np.uint32).reshape(-1, WORDS)
+    lo = (a & 0xFFFF).astype(np.uint16).view(np.int16)
+    hi = (a >> 16).astype(np.uint16).view(np.int16)
+    q = np.empty((len(a), 730), np.int16)
+    q[:, 0::2] = lo
+    q[:, 1::2] = hi
+    return q[:, :729]

@@ -225,6 +225,7 @@ class SolidBuilder:
         self.cpieces = []
         self.pcurves = []
         self._keep = []
+        self._desc = None
 
     # vertices and edges
     def vertex(self, p):
@@ -294,6 +295,11 @@ class SolidBuilder:
         self.faces[face]["loops"].append(uses)
 
     def desc(self) -> IcamSolidDesc:
+        if getattr(self, "_desc", None) is not None:
+            return self._desc
+        for e in self.edges:
+            e.f0 = e.f1 = -1
+        self.pcurves = []
         faces = (IcamFaceDesc * len(self.faces))()
         uses = []
         for fi, fd in enumerate(self.faces):

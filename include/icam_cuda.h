@@ -1,0 +1,142 @@
+/*
+ * icam_cuda.h — the C ABI of the B200 exact part field.
+ *
+ * These entry points replace the reference's GPU host for the part field,
+ * `PartGpu` (crates/icam-sim/src/partgpu.rs), and the level bake of its brick
+ * cache, `PartCache::level` (crates/icam-sim/src/partcache.rs:433-506). Every
+ * argument is a plain pointer or size: the caller owns all host arrays, the
+ * library owns the device memory inside an IcamPack. Each pack has its own CUDA
+ * stream; calls on one pack must not overlap (serialise them, as the reference
+ * serialises its dispatches on one queue).
+ *
+ * Values follow the reference kernel's contract (crates/icam-core/src/solid3/
+ * gpu.wgsl:1909-1921): each node or point comes back as (value, flag) with flag
+ * 0 = the exact signed distance, 1 = only a lower bound past the clamp is known
+ * (value = that bound, its sign to come from a neighbour), 2 = undecided.
+ *
+ * The brick layout is the reference's (crates/icam-sweep/src/cache.rs:69-92):
+ * 8 x 8 x 8 cells, 9 x 9 x 9 nodes x fastest, each stored as
+ * round(clamp(d / clamp, -1, 1) * 32767) in an i16, two to a 32-bit word low half
+ * first, 365 words a brick; the map holds a slot or ICAM_AIR / ICAM_SOLID.
+ */
+#ifndef ICAM_CUDA_H
+#define ICAM_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "icam_solid.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ICAM_AIR 0xffffffffu   /* cache.rs:84 AIR */
+#define ICAM_SOLID 0xfffffffeu /* cache.rs:85 SOLID */
+#define ICAM_WORDS 365         /* cache.rs:91 WORDS */
+#define ICAM_NODES 729
+
+/* Arithmetic of the per-node evaluation. */
+enum {
+  ICAM_FP64 = 0,          /* every step in double precision */
+  ICAM_MIXED = 1,         /* single-precision bulk, double-precision polish, trim near loops and signs */
+  ICAM_MIXED_LEARNED = 2  /* ICAM_MIXED seeded by the pack's trained seed network */
+};
+
+/* Status codes. */
+enum {
+  ICAM_OK = 0,
+  ICAM_ERR_ARG = 1,     /* a bad argument (message in err) */
+  ICAM_ERR_CUDA = 2,    /* a CUDA call failed */
+  ICAM_ERR_PACK = 3,    /* the solid could not be packed */
+  ICAM_ERR_ROOM = 7,    /* a device work list overflowed (gpu.wgsl why-code 7) */
+  ICAM_ERR_BUDGET = 8   /* a bounded device loop gave up (gpu.wgsl why-code 8) */
+};
+
+typedef struct IcamPack IcamPack;
+
+typedef struct IcamPackOptions {
+  int device;    /* CUDA device ordinal */
+  double need;   /* distance (mm) within which B-spline sub-patches should certify */
+} IcamPackOptions;
+
+typedef struct IcamBakeStats {
+  int64_t boxes_read;      /* box centres read by the decision */
+  int64_t bricks_read;     /* bricks whose nodes were read */
+  int64_t bricks_words;    /* of those, bricks stored as words (not air or solid) */
+  int64_t nodes_exact;     /* flag 0 nodes */
+  int64_t nodes_far;       /* flag 1 nodes, signed by the fill */
+  int64_t nodes_undecided; /* flag 2 nodes left after the device fallback (bridged) */
+  int64_t pairs;           /* (brick, candidate) pairs evaluated */
+  int64_t fallback_nodes;  /* nodes sent to the subdivision fallback */
+  int64_t kernel_launches; /* kernels launched by the call */
+  double ms_decide, ms_cull, ms_nodes, ms_post; /* device time by stage */
+} IcamBakeStats;
+
+/* Packs the solid for the device (PartGpu::new, partgpu.rs:132; Exact::gpu_pack,
+ * crates/icam-core/src/solid3/gpu.rs:259). Returns ICAM_OK and *out, or an error
+ * with a message in err. */
+int icam_pack_create(const IcamSolidDesc* solid, const IcamPackOptions* opt, IcamPack** out, char* err,
+                     size_t errlen);
+
+void icam_pack_destroy(IcamPack* pack);
+
+/* Counts of what the pack holds: faces, edges, vertices, B-spline sub-patches,
+ * edge pieces, trim cells, tree nodes. */
+int icam_pack_info(const IcamPack* pack, int64_t counts[7]);
+
+/* Signed distance of n points (x, y, z), each (value, flag) as above. With
+ * capped != 0 a point needs an exact value only within `clamp` (past it the
+ * answer may be the bound, flag 1), as PartGpu::points_scatter_capped
+ * (partgpu.rs:249); with capped == 0 every point is read exactly
+ * (PartGpu::points_refined, partgpu.rs:243). Host arrays. */
+int icam_points(IcamPack* pack, const double* xyz, size_t n, double clamp, int capped, int precision,
+                double* value_out, int8_t* flag_out);
+
+/* The 729 nodes of each brick whose first node is first_nodes[i] (cell side h),
+ * exact within `clamp` (PartGpu::bricks / bricks_scatter, partgpu.rs:227-241):
+ * values_out n x 729 (value, flag) as float pairs, as the reference returns them;
+ * d_out (optional) the same values in double. Candidates are listed on the device
+ * (the reference lists them on the CPU, GpuPack::list, gpu.rs:709). */
+int icam_bricks(IcamPack* pack, const double* first_nodes, size_t n, double h, double clamp, int precision,
+                float* values_out, double* d_out);
+
+/* One level of the brick cache (PartCache::level, partcache.rs:433): bricks of
+ * 8 x 8 x 8 cells of side h, the first node at lo, nb bricks along each axis,
+ * the box grid aligned on `origin` (the stock's low corner; partcache.rs:250-259),
+ * values clamped to `clamp` (h sqrt(3) in the reference). Decides every brick on
+ * the device (partcache.rs:226-331), reads the others' nodes, signs the far nodes,
+ * bridges the undecided ones, quantises and packs them (partcache.rs:759-970).
+ * map_out: nb[0]*nb[1]*nb[2] entries, x fastest (slot, ICAM_AIR or ICAM_SOLID);
+ * atlas_out: up to atlas_cap_words words, slots of 365 words in brick order;
+ * *n_slots: the slots written. A NULL atlas_out returns *n_slots only. */
+int icam_bake_level(IcamPack* pack, double h, const double lo[3], const int64_t nb[3], double clamp,
+                    const double origin[3], int precision, uint32_t* map_out, uint32_t* atlas_out,
+                    size_t atlas_cap_words, size_t* n_slots, IcamBakeStats* stats);
+
+/* The same bake, its results left in device memory the pack owns (valid until the
+ * next bake on the pack): *d_map and *d_atlas are device pointers. For callers
+ * that consume the level on the GPU (the reference's viewer uploads it to its ray
+ * caster). */
+int icam_bake_level_device(IcamPack* pack, double h, const double lo[3], const int64_t nb[3], double clamp,
+                           const double origin[3], int precision, const uint32_t** d_map,
+                           const uint32_t** d_atlas, size_t* n_slots, IcamBakeStats* stats);
+
+/* The candidate features within reach of a point's box, as the device lists them
+ * (PartGpu::list, partgpu.rs:220): codes kind << 28 | index (kinds: 0 analytic
+ * face, 1 B-spline sub-patch, 2 line or arc edge, 3 spline edge piece, 4 vertex).
+ * Host-only, reentrant. */
+int icam_list(const IcamPack* pack, const double c[3], double r, double d, uint32_t* codes, size_t cap,
+              size_t* n);
+
+/* Keeps the device busy for `secs` so its clocks are up (PartGpu::warm, partgpu.rs:188). */
+int icam_warm(IcamPack* pack, double secs);
+
+/* The last error message of a call on this pack. */
+const char* icam_last_error(const IcamPack* pack);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ICAM_CUDA_H */

@@ -20,6 +20,9 @@ static void bern3(double t, double b[4]) {
 
 // The rational coordinate k of a piece at t (b_eval of trim2.rs on a rational piece).
 double tp_eval(const TPiece& p, int k, double t) {
+  // trim2.rs:135-139 b_eval: a constant is itself
+  double e0 = p.c[0][k] / p.c[0][2];
+  if (e0 == p.c[1][k] / p.c[1][2] && e0 == p.c[2][k] / p.c[2][2] && e0 == p.c[3][k] / p.c[3][2]) return e0;
   double b[4];
   bern3(t, b);
   double n = 0, w = 0;
