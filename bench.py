@@ -1,0 +1,274 @@
+#!/usr/bin/env python3
+"""Benchmark of the exact part field's narrow-band brick bake on B200.
+
+Workload (one step): the level bake of the brick cache (the reference's
+PartCache::level, crates/icam-sim/src/partcache.rs:433) of the freeform-top part —
+a 120 x 120 x 50 mm block whose top is a clamped bicubic rational B-spline with
+16 x 16 control points (8 seeded Gaussian bumps, weights in [0.8, 1.2]) — at
+h = 0.1 mm with a narrow band of +-2 mm (the clamp: every node within 2 mm of the
+surface exact, the rest clamped), over the part's box grown by the band. A voxel is
+a cell of a brick the bake reads (512 a brick). Under torchrun each rank bakes its
+own part (seed = rank): weak scaling, no collective on the data path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed|learned]
+    python bench.py --impl reference ...   # the reference's CPU path (the oracle port)
+
+Prints one JSON line (rank 0).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "narrow-band SDF voxels/s, mixed+learned vs plain FP64 kernel, err ≤1e-7·diag"
+H = 0.1
+BAND = 2.0
+# algorithmic FLOPs a node spends on one candidate of each kind (analytic face,
+# B-spline span, line or arc edge, spline edge piece, vertex): foot + uv + one parity
+# leg; 6 Newton steps of 750 + trim 200; closed-form foot; 6 steps of 120; a distance
+FLOPS_PER_CANDIDATE = np.array([80.0, 6 * 750.0 + 200.0, 40.0, 6 * 120.0, 10.0])
+
+
+def workload(seed: int):
+    from implicitcam_b200 import parts
+
+    b = parts.freeform_top(seed=seed)
+    # the part's box: the control net's box (the top is within its control points)
+    pts = np.asarray(b.verts)
+    net = np.concatenate([np.asarray(p).reshape(-1, 4) for p in b.patches])
+    xyz = net[:, :3] / net[:, 3:]
+    lo = np.minimum(pts.min(0), xyz.min(0))
+    hi = np.maximum(pts.max(0), xyz.max(0))
+    lo = lo - BAND
+    nb = np.ceil((hi + BAND - lo) / (8 * H)).astype(np.int64)
+    return b, lo, nb
+
+
+def sample_clocks(path):
+    q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+    try:
+        return subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200"],
+                                stdout=open(path, "w"), stderr=subprocess.DEVNULL)
+    except OSError:
+        return None
+
+
+def read_clocks(path, device):
+    sm, mx, reasons = [], 0.0, set()
+    try:
+        for line in open(path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9 or f[0] != str(device):
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"], f[5:9]):
+                if v.lower() in ("active", "0x1", "1"):
+                    reasons.add(name)
+    except OSError:
+        pass
+    return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None, "reasons": sorted(reasons),
+            "samples": len(sm)}
+
+
+def cpu_bake_sample(seed, bricks_target_s=12.0, threads=None):
+    """The oracle's bake (the reference's exact_brick, partcache.rs:979) of a sample of
+    the level's read bricks on all host cores: voxels/s, cores, sample text."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import icam_oracle
+
+    b, lo, nb = workload(seed)
+    o = icam_oracle.Oracle(b, threads=threads)
+    rng = np.random.default_rng(seed)
+    # bricks the bake reads: those holding random points of the freeform top (every
+    # brick the surface passes through is read)
+    pa = np.asarray(b.patches[0]).reshape(13, 13, 4, 4, 4)
+    k = 4096
+    ia, ib = rng.integers(0, 13, k), rng.integers(0, 13, k)
+    s, t = rng.uniform(0, 1, k), rng.uniform(0, 1, k)
+    bs = np.stack([(1 - s) ** 3, 3 * (1 - s) ** 2 * s, 3 * (1 - s) * s * s, s ** 3], 1)
+    bt = np.stack([(1 - t) ** 3, 3 * (1 - t) ** 2 * t, 3 * (1 - t) * t * t, t ** 3], 1)
+    hom = np.einsum("ki,kj,kijc->kc", bs, bt, pa[ia, ib])
+    xyz = hom[:, :3] / hom[:, 3:]
+    cell = np.floor((xyz - lo) / (8 * H)).astype(np.int64)
+    firsts = lo + 8 * H * np.unique(cell, axis=0)
+    firsts = firsts[rng.permutation(len(firsts))]
+    n = 8
+    t0 = time.perf_counter()
+    o.bricks(firsts[:n], H, BAND)
+    dt = time.perf_counter() - t0
+    n2 = int(max(n, min(len(firsts), n * bricks_target_s / max(dt, 1e-3))))
+    t0 = time.perf_counter()
+    o.bricks(firsts[:n2], H, BAND)
+    dt = time.perf_counter() - t0
+    return 512.0 * n2 / dt, o.threads, f"{n2} random read bricks of the top's window (h={H}, clamp={BAND}), {dt:.1f} s"
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    vals = []
+    for _ in range(args.warmup):
+        cpu_bake_sample(0, bricks_target_s=2.0)
+    for _ in range(args.steps):
+        v, cores, sample = cpu_bake_sample(0, bricks_target_s=8.0)
+        vals.append(v)
+    value = float(np.mean(vals))
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "voxels/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"freeform-top level bake, h={H} mm, band +-{BAND} mm", "seed": 0},
+        "cpu_baseline": {"value": value, "unit": "voxels/s", "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "voxels/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed", "learned"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from implicitcam_b200 import part_gpu
+
+    prec = {"fp64": part_gpu.FP64, "mixed": part_gpu.MIXED, "learned": part_gpu.MIXED_LEARNED}[args.precision]
+    b, lo, nb = workload(seed=rank)
+    need = BAND + 8 * H * np.sqrt(3.0)
+    g = part_gpu.PartGpu(b, need=need, device=local)
+    stream = torch.cuda.ExternalStream(g.stream(), device=local)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")  # > L2 (126 MB)
+
+    def step(device_only=True, host=None):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        if device_only:
+            _, _, ns, st = g.level_device(H, lo, nb, BAND, precision=prec)
+        else:
+            m, a = host
+            ns, st = g.level_into(H, lo, nb, BAND, m, a, precision=prec)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1), ns, st
+
+    for _ in range(args.warmup):
+        step()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk_path = os.path.join(tempfile.gettempdir(), f"icam_clocks_{os.getpid()}.csv")
+    smi = sample_clocks(clk_path) if rank == 0 else None
+    ms, stats = [], []
+    for _ in range(args.steps):
+        t, ns, st = step()
+        ms.append(t)
+        stats.append(st)
+    torch.cuda.synchronize()
+    if smi:
+        smi.terminate()
+        smi.wait()
+    total_ms = float(sum(ms))
+    voxels = 512.0 * stats[-1]["bricks_read"]
+    if dist:
+        t = torch.tensor([total_ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        v = torch.tensor([voxels], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(v)
+        voxels = float(v.item())
+        dist.barrier()
+    value = voxels * args.steps / (total_ms * 1e-3)
+    # end to end through the C ABI: the map and atlas read back into pinned host memory
+    m_host = torch.empty(int(np.prod(nb)), dtype=torch.int32, pin_memory=True)
+    a_host = torch.empty((max(stats[-1]["bricks_words"], 1) * part_gpu.WORDS,), dtype=torch.int32, pin_memory=True)
+    e2e_ms = []
+    for _ in range(max(1, args.steps)):
+        t, ns, st = step(device_only=False, host=(m_host, a_host))
+        e2e_ms.append(t)
+    e2e_total = float(sum(e2e_ms))
+    if dist:
+        t = torch.tensor([e2e_total], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e_value = voxels * len(e2e_ms) / (e2e_total * 1e-3)
+    d2h = int(np.prod(nb)) * 4 + stats[-1]["bricks_words"] * part_gpu.WORDS * 4
+    if rank == 0:
+        st = stats[-1]
+        node_ms = float(np.mean([s["ms_nodes"] for s in stats]))
+        census = np.array(st["census"], dtype=np.float64)
+        flops = 729.0 * float(census @ FLOPS_PER_CANDIDATE)
+        peak = g.probe_fma(part_gpu.FP64 if prec == part_gpu.FP64 else part_gpu.MIXED)
+        achieved = flops / (node_ms * 1e-3)
+        cpu = None
+        if not args.no_cpu and world == 1:
+            v, cores, sample = cpu_bake_sample(0)
+            cpu = {"value": v, "unit": "voxels/s", "cores": cores, "kind": "port", "sample": sample}
+        clocks = read_clocks(clk_path, local)
+        out = {
+            "metric": METRIC, "value": value, "unit": "voxels/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == part_gpu.FP64 else "f32+f64",
+            "data": "synthetic",
+            "config": {"workload": f"freeform-top level bake, h={H} mm, band +-{BAND} mm", "part": "freeform_top",
+                       "seed": "rank", "h_mm": H, "band_mm": BAND, "nb": nb.tolist(), "precision": args.precision,
+                       "l2": "flushed (256 MB write) before every step"},
+            "bricks_read": st["bricks_read"], "bricks_stored": st["bricks_words"],
+            "nodes_exact": st["nodes_exact"], "nodes_undecided": st["nodes_undecided"],
+            "stage_ms": {"decide": st["ms_decide"], "nodes": st["ms_nodes"], "assemble": st["ms_post"]},
+            "gpu_launches": int(st["kernel_launches"]) * args.steps,
+            "e2e": {"value": e2e_value, "unit": "voxels/s", "h2d_bytes_per_step": 512,
+                    "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "fp64" if prec == part_gpu.FP64 else "fp32", "kernel": "k_bricks",
+                         "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "peak_source": "measured FMA probe of this run (MEASURED_PEAKS.json holds no FP64/FP32 figure)",
+                         "algorithmic_flops_per_launch": flops},
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+        }
+        print(json.dumps(out), flush=True)
+    g.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

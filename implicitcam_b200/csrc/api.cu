@@ -196,6 +196,8 @@ int icam_pack_info(const IcamPack* pk, int64_t counts[7]) {
 
 const char* icam_last_error(const IcamPack* pk) { return pk ? pk->err.c_str() : "null pack"; }
 
+void* icam_pack_stream(const IcamPack* pk) { return pk ? static_cast<void*>(pk->stream) : nullptr; }
+
 int icam_points(IcamPack* pk, const double* xyz, size_t n, double clamp, int capped, int precision,
                 double* value_out, int8_t* flag_out) {
   if (!pk || (!xyz && n) || (!value_out && n) || (!flag_out && n)) return fail(pk, ICAM_ERR_ARG, "null argument");
@@ -416,6 +418,7 @@ static int bake_level(IcamPack* pk, double h, const double lo[3], const int64_t 
     stats->nodes_far = R ? int64_t(st[1]) : 0;
     stats->nodes_undecided = R ? int64_t(st[2]) : 0;
     stats->pairs = R ? int64_t(st[4]) : 0;
+    for (int k = 0; k < 5; k++) stats->census[k] = R ? int64_t(st[6 + k]) : 0;
     stats->kernel_launches = launches;
     float ms;
     cudaEventElapsedTime(&ms, ev[0], ev[1]);
@@ -495,6 +498,37 @@ int icam_list(const IcamPack* pk, const double c[3], double r, double d, uint32_
     }
   }
   *n = k;
+  return ICAM_OK;
+}
+
+int icam_probe_fma(IcamPack* pk, int precision, double* flops) {
+  if (!pk || !flops) return ICAM_ERR_ARG;
+  CK(cudaSetDevice(pk->device));
+  int sms = 0;
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, pk->device));
+  void* d;
+  int r;
+  if ((r = scratch(pk, 0, 64, &d))) return r;
+  const int blocks = sms * 8, threads = 256, iters = 1 << 14;
+  cudaEvent_t a, b;
+  CK(cudaEventCreate(&a));
+  CK(cudaEventCreate(&b));
+  float best = 1e30f;
+  for (int rep = 0; rep < 5; rep++) {
+    CK(cudaEventRecord(a, pk->stream));
+    if (precision == ICAM_FP64)
+      k_fma<double><<<blocks, threads, 0, pk->stream>>>((double*)d, iters);
+    else
+      k_fma<float><<<blocks, threads, 0, pk->stream>>>((float*)d, iters);
+    CK(cudaEventRecord(b, pk->stream));
+    CK(cudaEventSynchronize(b));
+    float ms;
+    CK(cudaEventElapsedTime(&ms, a, b));
+    if (rep > 0) best = std::min(best, ms);
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  *flops = 2.0 * 8.0 * double(iters) * blocks * threads / (best * 1e-3);
   return ICAM_OK;
 }
 

@@ -263,6 +263,24 @@ __global__ void __launch_bounds__(BRICK_THREADS) k_bricks(BrickArgs a) {
       atomicAdd((unsigned long long*)&a.stats[2], (unsigned long long)s_cnt[2]);
       atomicAdd((unsigned long long*)&a.stats[3], (unsigned long long)s_cnt[3]);
       atomicAdd((unsigned long long*)&a.stats[4], (unsigned long long)n);
+      // the census by kind, B-spline sub-patches counted by their distinct spans
+      unsigned long long kinds[5] = {0, 0, 0, 0, 0};
+      for (int k = 0; k < n; k++) {
+        uint32_t kind = s_code[k] >> IK_SHIFT;
+        if (kind == IK_SUB) {
+          const DSub& s = P.subs[s_code[k] & IK_MASK];
+          bool seen = false;
+          for (int j = 0; j < k && !seen; j++)
+            if ((s_code[j] >> IK_SHIFT) == IK_SUB) {
+              const DSub& o = P.subs[s_code[j] & IK_MASK];
+              seen = o.nurbs == s.nurbs && o.span_a == s.span_a && o.span_b == s.span_b;
+            }
+          if (!seen) kinds[1]++;
+        } else {
+          kinds[kind == IK_FACE ? 0 : kind == IK_EDGE ? 2 : kind == IK_PIECE ? 3 : 4]++;
+        }
+      }
+      for (int k = 0; k < 5; k++) atomicAdd((unsigned long long*)&a.stats[6 + k], kinds[k]);
       if (overflow) atomicAdd((unsigned long long*)&a.stats[5], 1ull);
     }
     __syncthreads();
@@ -376,6 +394,24 @@ __global__ void k_is_words(const int32_t* kind, int64_t n, int64_t* flag) {
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
     flag[i] = kind[i] == 0 ? 1 : 0;
 }
+
+// Independent FMA chains, eight a thread, for the throughput probe.
+template <class T>
+__global__ void k_fma(T* out, int iters) {
+  T a[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) a[k] = T(threadIdx.x + k);
+  const T m = T(0.999999), c = T(1e-7);
+  for (int i = 0; i < iters; i++)
+#pragma unroll
+    for (int k = 0; k < 8; k++) a[k] = a[k] * m + c;
+  T s = 0;
+#pragma unroll
+  for (int k = 0; k < 8; k++) s += a[k];
+  if (s == T(-1)) out[0] = s;
+}
+template __global__ void k_fma<double>(double*, int);
+template __global__ void k_fma<float>(float*, int);
 
 __global__ void k_warm(float* out, int iters) {
   float x = float(threadIdx.x);

@@ -58,5 +58,7 @@ __global__ void k_assemble(const int64_t* idx, const int32_t* kind, const int64_
                            const uint32_t* words, uint32_t* map, uint32_t* atlas);
 __global__ void k_is_words(const int32_t* kind, int64_t n, int64_t* flag);
 __global__ void k_warm(float* out, int iters);
+template <class T>
+__global__ void k_fma(T* out, int iters);
 
 }  // namespace icam

@@ -33,10 +33,13 @@ class IcamBakeStats(C.Structure):
         ("nodes_exact", C.c_int64), ("nodes_far", C.c_int64), ("nodes_undecided", C.c_int64),
         ("pairs", C.c_int64), ("fallback_nodes", C.c_int64), ("kernel_launches", C.c_int64),
         ("ms_decide", C.c_double), ("ms_cull", C.c_double), ("ms_nodes", C.c_double), ("ms_post", C.c_double),
+        ("census", C.c_int64 * 5),
     ]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_}
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "census"}
+        d["census"] = list(self.census)
+        return d
 
 
 def lib():
@@ -61,6 +64,9 @@ def lib():
                                              C.POINTER(vp), C.POINTER(sz), vp]
         L.icam_list.argtypes = [vp, vp, C.c_double, C.c_double, vp, sz, C.POINTER(sz)]
         L.icam_warm.argtypes = [vp, C.c_double]
+        L.icam_pack_stream.restype = vp
+        L.icam_pack_stream.argtypes = [vp]
+        L.icam_probe_fma.argtypes = [vp, C.c_int, C.POINTER(C.c_double)]
         _lib = L
     return _lib
 
@@ -148,6 +154,26 @@ class PartGpu:
                                           _p(a), a.size, C.byref(ns), C.byref(st)), "icam_bake_level")
         return m, a, st.as_dict()
 
+    def level_into(self, h, lo, nb, clamp, map_out, atlas_out, origin=None, precision=FP64):
+        """The bake with its map and atlas written into caller buffers (numpy arrays or
+        host torch tensors, pinned for fast copies): (slots, stats)."""
+        lo = np.ascontiguousarray(lo, dtype=np.float64)
+        nb = np.ascontiguousarray(nb, dtype=np.int64)
+        org = None if origin is None else np.ascontiguousarray(origin, dtype=np.float64)
+
+        def ptr(x):
+            return C.c_void_p(x.data_ptr()) if hasattr(x, "data_ptr") else _p(x)
+
+        def words(x):
+            return x.numel() if hasattr(x, "numel") else x.size
+
+        ns = C.c_size_t()
+        st = IcamBakeStats()
+        self._check(lib().icam_bake_level(self.h, float(h), _p(lo), _p(nb), float(clamp), _p(org), precision,
+                                          ptr(map_out), ptr(atlas_out), words(atlas_out), C.byref(ns), C.byref(st)),
+                    "icam_bake_level")
+        return ns.value, st.as_dict()
+
     def level_device(self, h, lo, nb, clamp=None, origin=None, precision=FP64):
         """The same bake with its results left on the device: (map ptr, atlas ptr, slots, stats)."""
         lo = np.ascontiguousarray(lo, dtype=np.float64)
@@ -168,6 +194,16 @@ class PartGpu:
         n = C.c_size_t()
         self._check(lib().icam_list(self.h, _p(c), float(r), float(d), _p(out), out.size, C.byref(n)), "icam_list")
         return out[: min(n.value, out.size)].copy()
+
+    def stream(self):
+        """The pack's CUDA stream handle (cudaStream_t as an int)."""
+        return lib().icam_pack_stream(self.h)
+
+    def probe_fma(self, precision=FP64):
+        """Measured FMA throughput of the device (FLOP/s) in double or single precision."""
+        f = C.c_double()
+        self._check(lib().icam_probe_fma(self.h, precision, C.byref(f)), "icam_probe_fma")
+        return f.value
 
     def warm(self, secs):
         self._check(lib().icam_warm(self.h, float(secs)), "icam_warm")

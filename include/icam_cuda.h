@@ -71,6 +71,11 @@ typedef struct IcamBakeStats {
   int64_t fallback_nodes;  /* nodes sent to the subdivision fallback */
   int64_t kernel_launches; /* kernels launched by the call */
   double ms_decide, ms_cull, ms_nodes, ms_post; /* device time by stage */
+  /* Candidates listed for the bricks read, summed over them, by kind as the
+   * reference's census counts them (Exact::near_kinds, solid3.rs:1727): analytic
+   * faces, B-spline spans (distinct spans of the sub-patches listed), line or arc
+   * edges, spline edge pieces, vertices. */
+  int64_t census[5];
 } IcamBakeStats;
 
 /* Packs the solid for the device (PartGpu::new, partgpu.rs:132; Exact::gpu_pack,
@@ -131,6 +136,16 @@ int icam_list(const IcamPack* pack, const double c[3], double r, double d, uint3
 
 /* Keeps the device busy for `secs` so its clocks are up (PartGpu::warm, partgpu.rs:188). */
 int icam_warm(IcamPack* pack, double secs);
+
+/* Measures the device's fused multiply-add throughput in double (precision
+ * ICAM_FP64) or single (ICAM_MIXED) precision: a kernel of independent FMA chains
+ * on every SM, timed with events on the pack's stream. *flops: FLOP/s (2 a FMA).
+ * No counterpart in the reference; the roofline denominators of the bench. */
+int icam_probe_fma(IcamPack* pack, int precision, double* flops);
+
+/* The CUDA stream (a cudaStream_t) the pack's calls run on, for callers that order
+ * their own work or events around them. */
+void* icam_pack_stream(const IcamPack* pack);
 
 /* The last error message of a call on this pack. */
 const char* icam_last_error(const IcamPack* pack);
