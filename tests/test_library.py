@@ -1,0 +1,66 @@
+"""The CUDA library as a C ABI, without a GPU: it loads, exports every entry point
+include/icam_cuda.h declares, checks its arguments, and fails loudly (an error code
+and message, never a CPU path) when no device is there."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from implicitcam_b200 import build, part_gpu, parts
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared():
+    src = open(os.path.join(ROOT, "include", "icam_cuda.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(icam_\w+)\s*\(", src)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    build.build()
+    return C.CDLL(part_gpu.LIB)
+
+
+def test_exports_every_declared_entry_point(lib):
+    names = declared()
+    assert len(names) >= 12, names
+    for n in names:
+        assert hasattr(lib, n), n
+
+
+def test_solid_descriptions_are_closed_shells():
+    for name, make in parts.CONFIGS.items():
+        b = make()
+        d = b.desc()
+        assert d.n_faces > 0 and d.n_edges > 0 and d.n_verts > 0, name
+        # every edge used by two faces (twice by one for a seam)
+        for i in range(d.n_edges):
+            e = d.edges[i]
+            assert e.f0 >= 0 and e.f1 >= 0, (name, i)
+
+
+def test_bad_arguments_are_refused(lib):
+    L = part_gpu.lib()
+    err = C.create_string_buffer(256)
+    h = C.c_void_p()
+    assert L.icam_pack_create(None, None, C.byref(h), err, 256) == 1
+    assert b"null" in err.value
+    assert L.icam_pack_info(None, None) == 1
+
+
+@pytest.mark.skipif(__import__("torch").cuda.is_available(), reason="a GPU is present")
+def test_no_gpu_fails_loudly():
+    with pytest.raises(part_gpu.IcamError) as e:
+        part_gpu.PartGpu(parts.block_with_hole())
+    assert "cuda" in str(e.value).lower()
+
+
+def test_rust_binding_names_match_the_header():
+    """INTEGRATION.md's extern block binds exactly the header's entry points."""
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    rust = sorted(set(re.findall(r"pub fn (icam_\w+)\(", text)))
+    assert rust == declared()
