@@ -40,6 +40,11 @@ BAND = 2.0
 FLOPS_PER_CANDIDATE = np.array([80.0, 6 * 750.0 + 200.0, 40.0, 6 * 120.0, 10.0])
 
 
+def set_level(h, band):
+    global H, BAND
+    H, BAND = h, band
+
+
 def workload(seed: int):
     from implicitcam_b200 import parts
 
@@ -149,7 +154,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed", "learned"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--h", type=float, default=H, help="cell side (mm); smaller cases for profiling")
+    ap.add_argument("--band", type=float, default=BAND, help="narrow band half-width (mm), the clamp")
     args = ap.parse_args()
+    set_level(args.h, args.band)
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local = int(os.environ.get("LOCAL_RANK", 0))
