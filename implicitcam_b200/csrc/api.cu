@@ -247,7 +247,7 @@ int icam_bricks(IcamPack* pk, const double* first_nodes, size_t n, double h, dou
   a.flag_out = (int8_t*)dflag;
   a.stats = pk->d_stats;
   CK(cudaMemsetAsync(pk->d_stats, 0, 16 * sizeof(unsigned long long), pk->stream));
-  k_bricks<<<grid_for(int64_t(n), 1), 256, 0, pk->stream>>>(a);
+  launch_bricks(a, grid_for(int64_t(n), 1), pk->stream);
   CK(cudaGetLastError());
   std::vector<double> v(n * 729);
   std::vector<int8_t> f(n * 729);
@@ -380,7 +380,7 @@ static int bake_level(IcamPack* pk, double h, const double lo[3], const int64_t 
     b.kind_out = (int32_t*)d_kind;
     b.stats = pk->d_stats;
     CK(cudaMemsetAsync(pk->d_stats, 0, 16 * sizeof(unsigned long long), s));
-    k_bricks<<<grid_for(R, 1), 256, 0, s>>>(b);
+    launch_bricks(b, grid_for(R, 1), s);
     launches++;
     CK(cudaGetLastError());
     CK(cudaEventRecord(ev[3], s));

@@ -363,6 +363,100 @@ HDI void newton_bicubic(const double4* cp, double3 p, double* ps_, double* pt_, 
   *pt_ = t;
 }
 
+// ---------------------------------------------------------------- single precision (mixed path)
+
+// The bicubic in floats over control points rebased to the sub-patch's centre: the
+// point and first and second derivatives, as eval_bicubic.
+struct SEf {
+  float3 p, ps, pt, pss, pst, ptt;
+};
+
+HD float3 f3(float x, float y, float z) { return make_float3(x, y, z); }
+HD float dotf(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+HD SEf eval_bicubic_f(const float4* cp, float s, float t) {
+  float su = 1.f - s, sv = 1.f - t;
+  float bu[4] = {su * su * su, 3.f * su * su * s, 3.f * su * s * s, s * s * s};
+  float du[4] = {-3.f * su * su, 3.f * su * su - 6.f * su * s, 6.f * su * s - 3.f * s * s, 3.f * s * s};
+  float ddu[4] = {6.f * su, 6.f * s - 12.f * su, 6.f * su - 12.f * s, 6.f * s};
+  float bv[4] = {sv * sv * sv, 3.f * sv * sv * t, 3.f * sv * t * t, t * t * t};
+  float dv[4] = {-3.f * sv * sv, 3.f * sv * sv - 6.f * sv * t, 6.f * sv * t - 3.f * t * t, 3.f * t * t};
+  float ddv[4] = {6.f * sv, 6.f * t - 12.f * sv, 6.f * sv - 12.f * t, 6.f * t};
+  float4 a0 = {0, 0, 0, 0}, a1 = a0, a2 = a0, a3 = a0, a4 = a0, a5 = a0;
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    float4 r0 = {0, 0, 0, 0}, r1 = r0, r2 = r0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      float4 c = cp[4 * i + j];
+      r0.x += bv[j] * c.x, r0.y += bv[j] * c.y, r0.z += bv[j] * c.z, r0.w += bv[j] * c.w;
+      r1.x += dv[j] * c.x, r1.y += dv[j] * c.y, r1.z += dv[j] * c.z, r1.w += dv[j] * c.w;
+      r2.x += ddv[j] * c.x, r2.y += ddv[j] * c.y, r2.z += ddv[j] * c.z, r2.w += ddv[j] * c.w;
+    }
+    a0.x += bu[i] * r0.x, a0.y += bu[i] * r0.y, a0.z += bu[i] * r0.z, a0.w += bu[i] * r0.w;
+    a1.x += du[i] * r0.x, a1.y += du[i] * r0.y, a1.z += du[i] * r0.z, a1.w += du[i] * r0.w;
+    a2.x += bu[i] * r1.x, a2.y += bu[i] * r1.y, a2.z += bu[i] * r1.z, a2.w += bu[i] * r1.w;
+    a3.x += ddu[i] * r0.x, a3.y += ddu[i] * r0.y, a3.z += ddu[i] * r0.z, a3.w += ddu[i] * r0.w;
+    a4.x += du[i] * r1.x, a4.y += du[i] * r1.y, a4.z += du[i] * r1.z, a4.w += du[i] * r1.w;
+    a5.x += bu[i] * r2.x, a5.y += bu[i] * r2.y, a5.z += bu[i] * r2.z, a5.w += bu[i] * r2.w;
+  }
+  float iw = 1.f / a0.w;
+  SEf e;
+  e.p = f3(a0.x * iw, a0.y * iw, a0.z * iw);
+  e.ps = f3((a1.x - e.p.x * a1.w) * iw, (a1.y - e.p.y * a1.w) * iw, (a1.z - e.p.z * a1.w) * iw);
+  e.pt = f3((a2.x - e.p.x * a2.w) * iw, (a2.y - e.p.y * a2.w) * iw, (a2.z - e.p.z * a2.w) * iw);
+  e.pss = f3((a3.x - 2.f * e.ps.x * a1.w - e.p.x * a3.w) * iw, (a3.y - 2.f * e.ps.y * a1.w - e.p.y * a3.w) * iw,
+             (a3.z - 2.f * e.ps.z * a1.w - e.p.z * a3.w) * iw);
+  e.pst = f3((a4.x - e.ps.x * a2.w - e.pt.x * a1.w - e.p.x * a4.w) * iw,
+             (a4.y - e.ps.y * a2.w - e.pt.y * a1.w - e.p.y * a4.w) * iw,
+             (a4.z - e.ps.z * a2.w - e.pt.z * a1.w - e.p.z * a4.w) * iw);
+  e.ptt = f3((a5.x - 2.f * e.pt.x * a2.w - e.p.x * a5.w) * iw, (a5.y - 2.f * e.pt.y * a2.w - e.p.y * a5.w) * iw,
+             (a5.z - 2.f * e.pt.z * a2.w - e.p.z * a5.w) * iw);
+  return e;
+}
+
+// The projected Newton of newton_bicubic in floats (rebased point p), to a step under
+// 1e-6 of the square; the double polish takes it from there.
+HDI void newton_bicubic_f(const float4* cp, float3 p, float* ps_, float* pt_, int iters) {
+  float s = *ps_, t = *pt_;
+  for (int it = 0; it < iters; it++) {
+    SEf e = eval_bicubic_f(cp, s, t);
+    float3 r = f3(e.p.x - p.x, e.p.y - p.y, e.p.z - p.z);
+    float g0 = dotf(e.ps, r), g1 = dotf(e.pt, r);
+    float jss = dotf(e.ps, e.ps), jst = dotf(e.ps, e.pt), jtt = dotf(e.pt, e.pt);
+    float h0 = jss + dotf(e.pss, r), h1 = jst + dotf(e.pst, r), h2 = jtt + dotf(e.ptt, r);
+    bool hold_s = (s <= 0.f && g0 > 0.f) || (s >= 1.f && g0 < 0.f);
+    bool hold_t = (t <= 0.f && g1 > 0.f) || (t >= 1.f && g1 < 0.f);
+    float ds, dt;
+    if (hold_s && hold_t) break;
+    if (hold_s) {
+      ds = 0.f;
+      dt = -g1 / (h2 > 0.f ? h2 : fmaxf(jtt, 1e-30f));
+    } else if (hold_t) {
+      ds = -g0 / (h0 > 0.f ? h0 : fmaxf(jss, 1e-30f));
+      dt = 0.f;
+    } else {
+      if (!(h0 > 0.f && h0 * h2 - h1 * h1 > 0.f)) {
+        h0 = jss;
+        h1 = jst;
+        h2 = jtt;
+      }
+      float det = h0 * h2 - h1 * h1;
+      if (fabsf(det) < 1e-30f) break;
+      float id = 1.f / det;
+      ds = -(h2 * g0 - h1 * g1) * id;
+      dt = -(h0 * g1 - h1 * g0) * id;
+    }
+    float ns = fminf(fmaxf(s + ds, 0.f), 1.f), nt = fminf(fmaxf(t + dt, 0.f), 1.f);
+    float moved = fabsf(ns - s) + fabsf(nt - t);
+    s = ns;
+    t = nt;
+    if (moved < 1e-6f) break;
+  }
+  *ps_ = s;
+  *pt_ = t;
+}
+
 // surface3.rs:565-572 critical
 HD bool is_critical(double3 p, const SE& e) {
   double3 r = e.p - p;

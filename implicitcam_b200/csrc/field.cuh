@@ -22,6 +22,7 @@ struct Acc {
   int nd;
   uint32_t dcode[8];
   double dlb[8];
+  bool record;  // only record a failing certificate's bound in und (the caller walks the tree later)
 };
 
 constexpr int MAX_DEFER = 8;
@@ -33,6 +34,7 @@ HD void acc_init(Acc& A, double cap) {
   A.why = 0;
   A.ub = INFINITY;
   A.nd = 0;
+  A.record = false;
 }
 
 // Lower bound on the distance from c to a feature, by kind (solid3.rs:1661-1690
@@ -300,6 +302,10 @@ HDI void subdivide(const DPack& P, uint32_t code, double3 p, Acc& A) {
 // Leaves a feature whose certificate fails at p for later (subdivided now when the
 // list is full).
 HDI void defer(const DPack& P, uint32_t code, double lb, double3 p, Acc& A) {
+  if (A.record) {
+    A.und = fmin(A.und, lb);
+    return;
+  }
   if (A.nd < MAX_DEFER) {
     A.dcode[A.nd] = code;
     A.dlb[A.nd] = lb;

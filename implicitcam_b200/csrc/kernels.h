@@ -1,6 +1,8 @@
 // Launch arguments of the field kernels (kernels.cu) and their declarations.
 #pragma once
 
+#include <cuda_runtime.h>
+
 #include <cstdint>
 
 #include "pack.h"
@@ -50,7 +52,16 @@ struct DecideArgs {
 };
 
 __global__ void k_points(DPack P, const double* xyz, int64_t n, double cap, double* value, int8_t* flag);
-__global__ void k_bricks(BrickArgs a);
+template <bool MIXED>
+__global__ void k_bricks_t(BrickArgs a);
+
+// The brick kernel in the pack's arithmetic.
+inline void launch_bricks(const BrickArgs& a, int grid, cudaStream_t s) {
+  if (a.mixed)
+    k_bricks_t<true><<<grid, 256, 0, s>>>(a);
+  else
+    k_bricks_t<false><<<grid, 256, 0, s>>>(a);
+}
 __global__ void k_decide(DecideArgs a);
 __global__ void k_gather_firsts(const int64_t* idx, int64_t n, int64_t nb0, int64_t nb1, double h, double lo0,
                                 double lo1, double lo2, double* firsts);

@@ -235,3 +235,39 @@ def test_full_size_bake_properties(torch_cuda, oracle_mod):
         d = o.sdf(c)[0]
         assert ((d > 0) == (val == part_gpu.AIR)).all()
     g.close()
+
+
+@pytest.mark.parametrize("name", ["block_with_hole", "bump_box", "freeform_top"])
+def test_mixed_level(torch_cuda, oracle_mod, name):
+    """The mixed-precision bake: the brick map (active set and AIR/SOLID signs) exactly
+    the oracle's, every stored value within one i16 step, no sign flip."""
+    b, g, o, lo, hi, diag = setup(name, oracle_mod)
+    h = 0.5 if name != "bump_box" else 0.125
+    l2, nb = level_params(lo, hi, h)
+    clamp = 2.0 if name == "freeform_top" else h * np.sqrt(3)
+    m, a, st = g.level(h, l2, nb, clamp, precision=part_gpu.MIXED)
+    om, oa, _, _ = oracle_level(o, oracle_mod, h, l2, nb, clamp)
+    assert st["nodes_undecided"] == 0
+    assert (m == om).all()
+    qg = part_gpu.unpack_atlas(a).astype(np.int64)
+    qo = part_gpu.unpack_atlas(oa).astype(np.int64)
+    assert np.abs(qg - qo).max() <= 1
+    assert not ((qg > 0) & (qo < 0)).any() and not ((qg < 0) & (qo > 0)).any()
+
+
+@pytest.mark.parametrize("name", ["block_with_hole", "freeform_top"])
+def test_mixed_brick_values(torch_cuda, oracle_mod, name):
+    """Values of the mixed kernel within 1e-7 of the diagonal of the oracle's."""
+    b, g, o, lo, hi, diag = setup(name, oracle_mod)
+    h = 0.5
+    l2, nb = level_params(lo, hi, h)
+    clamp = 2.0
+    _, _, firsts, f = oracle_level(o, oracle_mod, h, l2, nb, clamp)
+    sel = firsts[:: max(1, len(firsts) // 300)]
+    fo = f[:: max(1, len(firsts) // 300)]
+    vals, d = g.bricks(sel, h, clamp, precision=part_gpu.MIXED)
+    flag = vals[:, :, 1]
+    ex = flag == 0
+    assert (flag != 2).all()
+    assert np.abs(d[ex] - fo[ex]).max() <= 1e-7 * diag
+    assert (np.abs(fo[flag == 1]) >= clamp * (1 - 1e-12)).all()
