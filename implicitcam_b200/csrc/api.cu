@@ -2,6 +2,7 @@
 // and the level bake of the brick cache, all on one CUDA stream per pack.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -548,3 +549,120 @@ int icam_warm(IcamPack* pk, double secs) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// The brick read without allocation (icam_bricks_static).
+//
+// icam_bricks grows the pack's scratch buffers with cudaMalloc / cudaFree when a
+// call asks for more bricks than any call before it, and converts the values in a
+// host std::vector. Some callers cannot have either: a machining simulation that
+// has reserved the GPU's memory for its stock model up front leaves nothing for the
+// library to take, and a control loop that reads bricks between its own
+// stream-ordered kernels cannot afford cudaFree, which waits for the whole device to
+// go idle. This variant runs the same brick kernel with every buffer it needs
+// (first nodes, node values and flags, the float pairs, the kernel's counters) in one
+// file-scope device array of fixed size, so a call allocates nothing, on the device
+// or on the host. The array holds at most ICAM_STATIC_BRICKS bricks (about 3 MB);
+// larger requests are refused, and the caller splits them.
+//
+// The array is one per device and every call on that device shares it: two calls
+// that overlap in time (from two threads, or on two packs of one device) race on it
+// and must be serialised by the caller. The kernel's counters are the only part that
+// must start at zero; each call clears them on the pack's stream before the kernel.
+// The first call on a device looks the array's address up (cudaGetSymbolAddress,
+// with that device current), which may load this library's device code; make that
+// first call before any stream capture.
+// ---------------------------------------------------------------------------
+
+namespace {
+
+constexpr size_t kStaticStats = 0;  // 16 counters of the brick kernel
+constexpr size_t kStaticFirst = 256;
+constexpr size_t kStaticD = kStaticFirst + size_t(ICAM_STATIC_BRICKS) * 3 * sizeof(double);
+constexpr size_t kStaticPairs = kStaticD + size_t(ICAM_STATIC_BRICKS) * ICAM_NODES * sizeof(double);
+constexpr size_t kStaticFlag = kStaticPairs + size_t(ICAM_STATIC_BRICKS) * ICAM_NODES * 2 * sizeof(float);
+constexpr size_t kStaticBytes = kStaticFlag + size_t(ICAM_STATIC_BRICKS) * ICAM_NODES;
+static_assert(kStaticFirst % 256 == 0 && kStaticD % 256 == 0 && kStaticPairs % 256 == 0 && kStaticFlag % 256 == 0,
+              "static scratch regions are 256-byte aligned");
+
+constexpr int kStaticDevices = 64;
+std::atomic<void*> g_static_addr[kStaticDevices];
+
+// (value, flag) float pairs from the double values and the flags, converted as
+// icam_bricks converts them on the host.
+__global__ void k_static_pairs(const double* d, const int8_t* f, int64_t m, float2* pairs) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < m; i += int64_t(gridDim.x) * blockDim.x)
+    pairs[i] = make_float2(float(d[i]), float(f[i]));
+}
+
+int static_fail(char* err, size_t errlen, int code, const char* what, const char* detail) {
+  if (err && errlen) std::snprintf(err, errlen, "icam_bricks_static: %s%s%s", what, detail ? ": " : "", detail ? detail : "");
+  return code;
+}
+
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticBytes];
+
+#define SCK(call)                                                                                \
+  do {                                                                                           \
+    cudaError_t e_ = (call);                                                                     \
+    if (e_ != cudaSuccess) return static_fail(err, errlen, ICAM_ERR_CUDA, #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+extern "C" int icam_bricks_static(IcamPack* pk, const double* first_nodes, size_t n, double h, double clamp,
+                                  int precision, float* values_out, double* d_out, char* err, size_t errlen) {
+  if (!pk || (!first_nodes && n)) return static_fail(err, errlen, ICAM_ERR_ARG, "null argument", nullptr);
+  if (!(h > 0) || !(clamp > 0)) return static_fail(err, errlen, ICAM_ERR_ARG, "h and clamp must be positive", nullptr);
+  if (precision < ICAM_FP64 || precision > ICAM_MIXED_LEARNED)
+    return static_fail(err, errlen, ICAM_ERR_ARG, "unknown precision", nullptr);
+  if (n > size_t(ICAM_STATIC_BRICKS)) {
+    char detail[96];
+    std::snprintf(detail, sizeof detail, "%zu bricks asked, at most %d per call", n, ICAM_STATIC_BRICKS);
+    return static_fail(err, errlen, ICAM_ERR_ROOM, "more bricks than the static scratch holds", detail);
+  }
+  if (pk->device < 0 || pk->device >= kStaticDevices)
+    return static_fail(err, errlen, ICAM_ERR_ARG, "device ordinal out of range", nullptr);
+  if (n == 0) return ICAM_OK;
+  SCK(cudaSetDevice(pk->device));
+  unsigned char* base = static_cast<unsigned char*>(g_static_addr[pk->device].load(std::memory_order_acquire));
+  if (!base) {
+    void* p = nullptr;
+    SCK(cudaGetSymbolAddress(&p, g_static_scratch));
+    g_static_addr[pk->device].store(p, std::memory_order_release);
+    base = static_cast<unsigned char*>(p);
+  }
+  auto* stats = reinterpret_cast<unsigned long long*>(base + kStaticStats);
+  auto* dfirst = reinterpret_cast<double*>(base + kStaticFirst);
+  auto* dval = reinterpret_cast<double*>(base + kStaticD);
+  auto* dpairs = reinterpret_cast<float2*>(base + kStaticPairs);
+  auto* dflag = reinterpret_cast<int8_t*>(base + kStaticFlag);
+  const int64_t m = int64_t(n) * ICAM_NODES;
+  SCK(cudaMemcpyAsync(dfirst, first_nodes, n * 3 * sizeof(double), cudaMemcpyHostToDevice, pk->stream));
+  SCK(cudaMemsetAsync(stats, 0, 16 * sizeof(unsigned long long), pk->stream));
+  BrickArgs a{};
+  a.P = pk->dev;
+  a.firsts = dfirst;
+  a.dcs = nullptr;
+  a.n = int64_t(n);
+  a.h = h;
+  a.clamp = clamp;
+  a.leaves = pk->leaves;
+  a.n_leaves = int32_t(pk->leaves_host.size());
+  a.mixed = precision != ICAM_FP64;
+  a.d_out = dval;
+  a.flag_out = dflag;
+  a.stats = stats;
+  launch_bricks(a, grid_for(int64_t(n), 1), pk->stream);
+  SCK(cudaGetLastError());
+  if (values_out) {
+    k_static_pairs<<<grid_for(m, 256), 256, 0, pk->stream>>>(dval, dflag, m, dpairs);
+    SCK(cudaGetLastError());
+    SCK(cudaMemcpyAsync(values_out, dpairs, size_t(m) * sizeof(float2), cudaMemcpyDeviceToHost, pk->stream));
+  }
+  if (d_out) SCK(cudaMemcpyAsync(d_out, dval, size_t(m) * sizeof(double), cudaMemcpyDeviceToHost, pk->stream));
+  SCK(cudaStreamSynchronize(pk->stream));
+  return ICAM_OK;
+}
+
+#undef SCK

@@ -106,6 +106,20 @@ int icam_points(IcamPack* pack, const double* xyz, size_t n, double clamp, int c
 int icam_bricks(IcamPack* pack, const double* first_nodes, size_t n, double h, double clamp, int precision,
                 float* values_out, double* d_out);
 
+/* icam_bricks without allocation. No counterpart in the reference: it is for
+ * callers that may not allocate device or host memory during the call (memory
+ * reserved up front for the stock model; a loop that cannot take the device-wide
+ * wait of cudaFree). Same kernel and outputs as icam_bricks, with every buffer in
+ * one fixed device array of the library (one per device, about 3 MB) that all
+ * calls on that device share: calls that overlap in time race on it. n above
+ * ICAM_STATIC_BRICKS is refused with ICAM_ERR_ROOM. The first call on a device
+ * resolves the array's address and may load the library's device code: make it
+ * before any stream capture. Errors are written to err (errlen bytes), not to the
+ * pack's message. */
+#define ICAM_STATIC_BRICKS 256
+int icam_bricks_static(IcamPack* pack, const double* first_nodes, size_t n, double h, double clamp, int precision,
+                       float* values_out, double* d_out, char* err, size_t errlen);
+
 /* One level of the brick cache (PartCache::level, partcache.rs:433): bricks of
  * 8 x 8 x 8 cells of side h, the first node at lo, nb bricks along each axis,
  * the box grid aligned on `origin` (the stock's low corner; partcache.rs:250-259),
