@@ -248,7 +248,7 @@ int icam_bricks(IcamPack* pk, const double* first_nodes, size_t n, double h, dou
   a.flag_out = (int8_t*)dflag;
   a.stats = pk->d_stats;
   CK(cudaMemsetAsync(pk->d_stats, 0, 16 * sizeof(unsigned long long), pk->stream));
-  launch_bricks(a, grid_for(int64_t(n), 1), pk->stream);
+  launch_bricks(a, pk->stream);
   CK(cudaGetLastError());
   std::vector<double> v(n * 729);
   std::vector<int8_t> f(n * 729);
@@ -381,7 +381,7 @@ static int bake_level(IcamPack* pk, double h, const double lo[3], const int64_t 
     b.kind_out = (int32_t*)d_kind;
     b.stats = pk->d_stats;
     CK(cudaMemsetAsync(pk->d_stats, 0, 16 * sizeof(unsigned long long), s));
-    launch_bricks(b, grid_for(R, 1), s);
+    launch_bricks(b, s);
     launches++;
     CK(cudaGetLastError());
     CK(cudaEventRecord(ev[3], s));
@@ -517,10 +517,7 @@ int icam_probe_fma(IcamPack* pk, int precision, double* flops) {
   float best = 1e30f;
   for (int rep = 0; rep < 5; rep++) {
     CK(cudaEventRecord(a, pk->stream));
-    if (precision == ICAM_FP64)
-      k_fma<double><<<blocks, threads, 0, pk->stream>>>((double*)d, iters);
-    else
-      k_fma<float><<<blocks, threads, 0, pk->stream>>>((float*)d, iters);
+    launch_fma(precision == ICAM_FP64, d, blocks, threads, iters, pk->stream);
     CK(cudaEventRecord(b, pk->stream));
     CK(cudaEventSynchronize(b));
     float ms;
@@ -653,7 +650,7 @@ extern "C" int icam_bricks_static(IcamPack* pk, const double* first_nodes, size_
   a.d_out = dval;
   a.flag_out = dflag;
   a.stats = stats;
-  launch_bricks(a, grid_for(int64_t(n), 1), pk->stream);
+  launch_bricks(a, pk->stream);
   SCK(cudaGetLastError());
   if (values_out) {
     k_static_pairs<<<grid_for(m, 256), 256, 0, pk->stream>>>(dval, dflag, m, dpairs);

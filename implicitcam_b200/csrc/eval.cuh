@@ -22,6 +22,8 @@ namespace icam {
 
 #define HD __host__ __device__ __forceinline__
 #define HDI __host__ __device__ inline
+// out of line: paths the hot loops seldom take, kept out of their instruction stream
+#define HDC __host__ __device__ inline __noinline__
 
 HD double3 mk(double x, double y, double z) { return make_double3(x, y, z); }
 HD double3 operator+(double3 a, double3 b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
@@ -200,7 +202,7 @@ HDI bool tp_cross(const double* c, const double* sh, int k, double x, double* to
 
 // trim2.rs:1192-1259 parity of the path a -> (a.u, b.v) -> b, symbolically raised by e
 // and moved right by e^2, against the instances in `among`.
-HDI bool trim_parity(const DPack& P, const double* a, const double* b, const int32_t* among, int count) {
+HDC bool trim_parity(const DPack& P, const double* a, const double* b, const int32_t* among, int count) {
   int n = 0;
   bool up = a[1] < b[1], right = a[0] < b[0];
   for (int i = 0; i < count; i++) {

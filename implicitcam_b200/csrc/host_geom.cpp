@@ -286,6 +286,20 @@ bool piece_bounds(const H cp[4], double* lam_out, double d2[3][2]) {
   return true;
 }
 
+// lam + sum_k min((C - p)_k C''_k) > 1e-6 lam with C - p over the box grown by `need`:
+// each component of C - p within [-(w_k + need), w_k + need].
+bool piece_certifies(const Cubic3& z, double need) {
+  double lam, d2[3][2];
+  if (!piece_bounds(z.c, &lam, d2)) return false;
+  Bx b = z.box();
+  double e = 0.0;
+  for (int k = 0; k < 3; k++) {
+    double w = b.hi[k] - b.lo[k] + need;
+    e -= w * std::max(std::fabs(d2[k][0]), std::fabs(d2[k][1]));
+  }
+  return lam + e > 1e-6 * lam;
+}
+
 void Cubic3::eval(double s, V* P, V* D1) const {
   double b[4], d[4], dd[4];
   bern3(s, b, d, dd);
@@ -328,6 +342,10 @@ double Cubic3::thickness() const {
 
 static const double REF_U = 0.5137, REF_V = 0.4871;  // trim2.rs:102
 static const int MAX_TREE_DEPTH = 10;                // trim2.rs:99
+// A cell with loop pieces in it is split down to this depth even when few pieces touch
+// it (the reference stops at four): a point's parity walk is then needed only within a
+// cell of the loops, 1/128 of the domain across, and the answer is the same.
+static const int MIN_MIXED_DEPTH = 7;
 
 double tp_coord(const TP& p, int k, double t) {
   // a constant coordinate is that constant exactly (trim2.rs:135-139)
@@ -644,7 +662,7 @@ void TrimTree::build_cell(int id, const std::vector<int>& cand, const std::vecto
     cells[id].kind = 0;
     return;
   }
-  if (depth >= MAX_TREE_DEPTH || touching.size() <= 4) {
+  if (depth >= MAX_TREE_DEPTH || (touching.size() <= 4 && depth >= MIN_MIXED_DEPTH)) {
     cells[id].kind = 1;
     cells[id].among = touching;
     return;

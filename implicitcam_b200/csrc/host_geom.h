@@ -92,6 +92,10 @@ struct Cubic3 {
   }
 };
 
+// Whether the piece's convexity certificate (the device's piece_convex) holds for every
+// point within `need` of its control-point box.
+bool piece_certifies(const Cubic3& z, double need);
+
 // ---------------------------------------------------------------- trim trees
 
 // A loop piece in a face's (u, v): rational cubic, (u w, v w, w).

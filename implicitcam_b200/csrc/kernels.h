@@ -30,7 +30,10 @@ struct BrickArgs {
   int8_t* flag_out;       // optional n x 729 flags
   uint32_t* words_out;    // optional n x 365 packed words
   int32_t* kind_out;      // optional n kinds (0 words, 1 air, 2 solid)
-  unsigned long long* stats;  // exact, far, undecided, bridged, pairs, overflows
+  // exact, far, undecided, bridged, pairs, overflows, census [6..10]; [15] the kernel's
+  // brick counter. Zeroed before each launch; null for none (bricks then taken in a
+  // fixed order).
+  unsigned long long* stats;
 };
 
 struct DecideArgs {
@@ -52,16 +55,10 @@ struct DecideArgs {
 };
 
 __global__ void k_points(DPack P, const double* xyz, int64_t n, double cap, double* value, int8_t* flag);
-template <bool MIXED>
-__global__ void k_bricks_t(BrickArgs a);
 
-// The brick kernel in the pack's arithmetic.
-inline void launch_bricks(const BrickArgs& a, int grid, cudaStream_t s) {
-  if (a.mixed)
-    k_bricks_t<true><<<grid, 256, 0, s>>>(a);
-  else
-    k_bricks_t<false><<<grid, 256, 0, s>>>(a);
-}
+// The brick kernel (bricks.cu) in the arithmetic a.mixed names, one warp a brick over a
+// grid sized for the current device.
+void launch_bricks(const BrickArgs& a, cudaStream_t s);
 __global__ void k_decide(DecideArgs a);
 __global__ void k_gather_firsts(const int64_t* idx, int64_t n, int64_t nb0, int64_t nb1, double h, double lo0,
                                 double lo1, double lo2, double* firsts);
@@ -69,7 +66,7 @@ __global__ void k_assemble(const int64_t* idx, const int32_t* kind, const int64_
                            const uint32_t* words, uint32_t* map, uint32_t* atlas);
 __global__ void k_is_words(const int32_t* kind, int64_t n, int64_t* flag);
 __global__ void k_warm(float* out, int iters);
-template <class T>
-__global__ void k_fma(T* out, int iters);
+// Independent FMA chains in doubles (fp64) or floats: the throughput probe.
+void launch_fma(bool fp64, void* out, int blocks, int threads, int iters, cudaStream_t s);
 
 }  // namespace icam

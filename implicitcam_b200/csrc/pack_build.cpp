@@ -305,6 +305,33 @@ bool build_pack(const IcamSolidDesc* d, double need, HostPack* hp, std::string* 
           stack.push_back(l);
         }
       }
+      // each flat piece halved (up to 5 times) until |C - p|^2 certifies convex for
+      // every p within `need` of it, so that points that near take one Newton solve
+      // instead of the subdivision search; the curve and its closest points are the
+      // same, the halves' ends only add points of it to try
+      {
+        std::vector<Cubic3> fine;
+        struct Part {
+          Cubic3 z;
+          int depth;
+        };
+        for (const Cubic3& z0 : flat) {
+          std::vector<Part> st{{z0, 0}};
+          while (!st.empty()) {
+            Part q = st.back();
+            st.pop_back();
+            if (q.depth >= 5 || piece_certifies(q.z, need)) {
+              fine.push_back(q.z);
+            } else {
+              Cubic3 l, r;
+              q.z.split(0.5, &l, &r);
+              st.push_back({r, q.depth + 1});
+              st.push_back({l, q.depth + 1});
+            }
+          }
+        }
+        flat.swap(fine);
+      }
       e.first_piece = int(P.pieces.size());
       e.n_pieces = int(flat.size());
       for (size_t k = 0; k < flat.size(); k++) {
