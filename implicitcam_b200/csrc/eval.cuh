@@ -255,6 +255,42 @@ HDI bool trim_inside(const DPack& P, const DFace& f, double u, double v) {
   return false;
 }
 
+// What trim_inside answers over a whole parameter box [blo, bhi] of a face without
+// periodic directions: 1 inside or 0 outside when every cell the box meets (closed
+// boxes, so a point on a split line counts for both sides) is a leaf without loop
+// pieces and they agree, -1 otherwise (the point test decides). Points reduced into the
+// domain as trim_inside reduces them.
+HDI int trim_box_class(const DPack& P, const DFace& f, const double blo[2], const double bhi[2]) {
+  if (f.trim < 0) return 1;
+  if (f.period[0] > 0.0 || f.period[1] > 0.0) return -1;
+  double lo[2], hi[2];
+  for (int k = 0; k < 2; k++) {
+    lo[k] = fmin(fmax(blo[k], f.lo[k]), f.hi[k]);
+    hi[k] = fmin(fmax(bhi[k], f.lo[k]), f.hi[k]);
+  }
+  int stack[48];
+  int sp = 0, answer = -2, visited = 0;
+  stack[sp++] = f.trim;
+  while (sp > 0) {
+    const DCell& c = P.cells[stack[--sp]];
+    if (++visited > 256 || c.kind == 1) return -1;
+    if (c.kind == 0) {
+      if (answer == -2)
+        answer = c.inside;
+      else if (answer != c.inside)
+        return -1;
+      continue;
+    }
+    for (int q = 0; q < 4; q++) {
+      const DCell& kc = P.cells[c.kids[q]];
+      if (kc.lo[0] > hi[0] || kc.hi[0] < lo[0] || kc.lo[1] > hi[1] || kc.hi[1] < lo[1]) continue;
+      if (sp >= 48) return -1;
+      stack[sp++] = c.kids[q];
+    }
+  }
+  return answer == -2 ? -1 : answer;
+}
+
 // ---------------------------------------------------------------- bicubic patches
 
 struct SE {
