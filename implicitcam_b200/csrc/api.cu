@@ -312,6 +312,8 @@ static int bake_level(IcamPack* pk, double h, const double lo[3], const int64_t 
   while (ncur > 0) {
     DecideArgs a{};
     a.P = pk->dev;
+    a.leaves = pk->leaves;
+    a.n_leaves = int32_t(pk->leaves_host.size());
     a.boxes = (const Box4*)d_cur;
     a.n = ncur;
     a.size = size;
@@ -327,7 +329,7 @@ static int bake_level(IcamPack* pk, double h, const double lo[3], const int64_t 
     a.read_cap = total;
     a.n_read = cnt + 1;
     CK(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), s));
-    k_decide<<<grid_for(ncur, 64), 64, 0, s>>>(a);
+    launch_decide(a, s);
     launches++;
     CK(cudaGetLastError());
     unsigned long long nn = 0;

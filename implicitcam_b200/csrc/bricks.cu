@@ -3,16 +3,12 @@
 // post-processing, partcache.rs:759-970).
 #include <type_traits>
 
-#include "field.cuh"
 #include "kernels.h"
+#include "warp_list.cuh"
 
 namespace icam {
 
-constexpr int WARPS = 4;    // bricks a block works on at once, one a warp
-constexpr int MAXC = 128;   // candidates a brick may list
-constexpr int MAXSUB = 32;  // sub-patches a brick seeds from its centre
-constexpr int FR = 64;      // tree nodes one level of the list's walk may hold
-constexpr unsigned FULL = 0xffffffffu;
+constexpr int WARPS = 4;  // bricks a block works on at once, one a warp
 
 // The 26 neighbours of node n inside the brick, in the reference's order (dk, dj, di
 // from -1 to 1, partcache.rs:829-839).
@@ -26,54 +22,6 @@ __device__ __forceinline__ int nb_of(int n, int k, double* dist) {
   return a + 9 * b + 81 * c;
 }
 
-// A node the candidate list could not settle (more candidates than the list holds, or a
-// feature whose certificate fails there): the whole tree walk with every fallback, out
-// of line so the common path keeps its registers.
-__device__ __noinline__ void node_fallback(const DPack& P, double3 p, double clamp, double* value, int* flag) {
-  Acc A;
-  point_query(P, p, clamp, A);
-  finish(A, clamp, value, flag);
-}
-
-// Edges, pieces and vertices: eval_item out of line (faces and sub-patches, the common
-// candidates, are evaluated in the kernel's own loop).
-__device__ __noinline__ void eval_item_cold(const DPack& P, uint32_t code, double3 p, Acc& A) {
-  eval_item(P, code, p, A, 0, 0.5, 0.5);
-}
-
-// A node's features whose certificate failed there (at most two), searched by
-// subdivision after every other candidate has tightened the bound, nearest bound
-// first (the deferral of the tree walk, restated for the list). Out of line too.
-__device__ __noinline__ void node_resolve(const DPack& P, double3 p, uint32_t c0, double l0, uint32_t c1, double l1,
-                                         int nd, double* best, double* sd, double* und) {
-  Acc B;
-  B.best = *best;
-  B.sd = *sd;
-  B.und = INFINITY;
-  B.why = 0;
-  B.ub = INFINITY;
-  B.nd = 0;
-  B.record = false;
-  if (nd == 2 && l1 < l0) {
-    uint32_t tc = c0;
-    c0 = c1, c1 = tc;
-    double tl = l0;
-    l0 = l1, l1 = tl;
-  }
-  if (l0 < B.best) subdivide(P, c0, p, B);
-  if (nd == 2 && l1 < B.best) subdivide(P, c1, p, B);
-  *best = B.best;
-  *sd = B.sd;
-  *und = B.und;
-}
-
-// A seeded sub-patch's solution at the brick's centre, for first-order seeds at the
-// nodes: (s, t) there, the inverse Hessian of |S - c|^2 and the tangents, so that
-// (s, t)(p) ~ (s, t) + H^-1 [S_s.(p - c), S_t.(p - c)].
-struct Seed {
-  double s, t, i00, i01, i11;
-  double ss[3], st[3];
-};
 
 // A warp's shared memory for its brick. The list before its ranking and the walk's
 // frontier share room with the node values, which come later.
@@ -219,94 +167,10 @@ __global__ void __launch_bounds__(WARPS * 32, 2) k_bricks_t(BrickArgs a) {
       continue;
     }
     // ---- 1. list
-    if (lane == 0) {
-      S.n = 0;
-      S.u.list.fr[0][0] = 0;
-    }
-    __syncwarp();
-    bool walked = true;
-    {
-      int cur = 0, ncur = 1;
-      while (ncur > 0) {
-        int nnext = 0;
-        for (int base = 0; base < ncur; base += 32) {
-          const int i = base + lane;
-          bool inner = false;
-          int32_t kid = 0;
-          if (i < ncur) {
-            const DBvh& nd = P.bvh[S.u.list.fr[cur][i]];
-            if (box_dist_f(c, nd.lo, nd.hi) <= reach) {
-              if (nd.count > 0) {
-                for (int k = 0; k < nd.count; k++) {
-                  uint32_t code = P.items[nd.first + k];
-                  double lb = item_lb(P, code, c);
-                  if (lb <= reach) {
-                    int slot = atomicAdd(&S.n, 1);
-                    if (slot < MAXC) {
-                      S.u.list.code[slot] = code;
-                      S.u.list.lb[slot] = lb;
-                    }
-                  }
-                }
-              } else {
-                inner = true;
-                kid = nd.first;
-              }
-            }
-          }
-          const unsigned m = __ballot_sync(FULL, inner);
-          const int off = nnext + 2 * __popc(m & ((1u << lane) - 1u));
-          if (inner && off + 1 < FR) {
-            S.u.list.fr[cur ^ 1][off] = kid;
-            S.u.list.fr[cur ^ 1][off + 1] = kid + 1;
-          }
-          nnext += 2 * __popc(m);
-        }
-        __syncwarp();
-        if (nnext > FR) {  // a level wider than the frontier: every leaf instead
-          walked = false;
-          break;
-        }
-        cur ^= 1;
-        ncur = nnext;
-      }
-    }
-    if (!walked) {
-      if (lane == 0) S.n = 0;
-      __syncwarp();
-      for (int leaf = lane; leaf < a.n_leaves; leaf += 32) {
-        const DBvh& nd = P.bvh[a.leaves[leaf]];
-        if (box_dist_f(c, nd.lo, nd.hi) > reach) continue;
-        for (int k = 0; k < nd.count; k++) {
-          uint32_t code = P.items[nd.first + k];
-          double lb = item_lb(P, code, c);
-          if (lb <= reach) {
-            int slot = atomicAdd(&S.n, 1);
-            if (slot < MAXC) {
-              S.u.list.code[slot] = code;
-              S.u.list.lb[slot] = lb;
-            }
-          }
-        }
-      }
-    }
-    __syncwarp();
-    int n = S.n;
+    int n = warp_list(P, a.leaves, a.n_leaves, c, reach, S.u.list.code, S.u.list.lb, S.u.list.fr, &S.n, lane);
     const bool overflow = n > MAXC;
     if (overflow) n = MAXC;
-    // rank sort: ties by code so the order does not depend on the list's arrival order
-    for (int k = lane; k < n; k += 32) {
-      double lb = S.u.list.lb[k];
-      uint32_t code = S.u.list.code[k];
-      int rank = 0;
-      for (int j = 0; j < n; j++) {
-        double l2 = S.u.list.lb[j];
-        rank += (l2 < lb) || (l2 == lb && S.u.list.code[j] < code);
-      }
-      S.code[rank] = code;
-      S.lb[rank] = lb;
-    }
-    __syncwarp();
+    warp_rank(S.u.list.code, S.u.list.lb, n, S.code, S.lb, lane);
     // ---- 2. certify and seed the first MAXSUB sub-patches, a lane each
     {
       int subs_before = 0;
@@ -325,26 +189,7 @@ __global__ void __launch_bounds__(WARPS * 32, 2) k_bricks_t(BrickArgs a) {
           cert = sub_convex(s, first, first + mk(8 * h, 8 * h, 8 * h)) ? 1 : 0;
           if (before < MAXSUB) {
             slot = before;
-            const double4* cp = P.sub_cp + 16 * size_t(idx);
-            double ss = 0.5, tt = 0.5;
-            bool conv;
-            newton_bicubic(cp, c, &ss, &tt, 12, &conv);
-            SE e = eval_bicubic(cp, ss, tt);
-            double3 r = e.p - c;
-            double h0 = dot(e.ps, e.ps) + dot(e.pss, r), h1 = dot(e.ps, e.pt) + dot(e.pst, r),
-                   h2 = dot(e.pt, e.pt) + dot(e.ptt, r);
-            if (!(h0 > 0.0 && h0 * h2 - h1 * h1 > 0.0)) h0 = dot(e.ps, e.ps), h1 = dot(e.ps, e.pt), h2 = dot(e.pt, e.pt);
-            double det = h0 * h2 - h1 * h1;
-            Seed sd;
-            sd.s = ss, sd.t = tt;
-            if (fabs(det) > 1e-300) {
-              sd.i00 = h2 / det, sd.i01 = -h1 / det, sd.i11 = h0 / det;
-            } else {
-              sd.i00 = sd.i01 = sd.i11 = 0.0;
-            }
-            sd.ss[0] = e.ps.x, sd.ss[1] = e.ps.y, sd.ss[2] = e.ps.z;
-            sd.st[0] = e.pt.x, sd.st[1] = e.pt.y, sd.st[2] = e.pt.z;
-            S.v.seed[slot] = sd;
+            S.v.seed[slot] = seed_at(P.sub_cp + 16 * size_t(idx), c);
           }
         } else if ((S.code[k] >> IK_SHIFT) == IK_FACE) {
           // a plane's trim over the feet of the whole brick (the box's corners projected,
@@ -373,131 +218,15 @@ __global__ void __launch_bounds__(WARPS * 32, 2) k_bricks_t(BrickArgs a) {
     __syncwarp();
     // ---- 3. every node: the warp's lanes walk the same ranked candidates together
     int cnt[3] = {0, 0, 0};
+    const WarpCands W{S.code, S.lb, S.cert, S.slot, S.v.seed, S.net, S.net32, n, overflow};
     for (int nn0 = 0; nn0 < 729; nn0 += 32) {
       const int nn = nn0 + lane;
       const bool live = nn < 729;
       double3 p = first + mk(h * (nn % 9), h * ((nn / 9) % 9), h * (nn / 81));
-      double rr = len(p - c);
-      double best = live ? clamp : -1.0;  // a lane past the last node is done
-      double sdv = NAN, und = INFINITY;
-      // features left for subdivision: the first two, and how many
-      uint32_t dc0 = 0, dc1 = 0;
-      double dl0 = 0.0, dl1 = 0.0;
-      int nd = 0;
-      auto defer_item = [&](uint32_t code, double lb) {
-        und = fmin(und, lb);
-        if (nd == 0)
-          dc0 = code, dl0 = lb;
-        else if (nd == 1)
-          dc1 = code, dl1 = lb;
-        nd++;
-      };
-      if (!overflow) {
-        for (int k = 0; k < n; k++) {
-          double lbc = S.lb[k];
-          if (__all_sync(FULL, lbc - rr >= best)) break;  // ranked: nothing later is nearer
-          uint32_t code = S.code[k];
-          uint32_t kind = code >> IK_SHIFT, idx = code & IK_MASK;
-          if (kind == IK_SUB) {  // the control net to shared memory, by the whole warp
-            __syncwarp();
-            if (lane < 16)
-              S.net[lane] = P.sub_cp[16 * size_t(idx) + lane];
-            else if (MIXED)
-              S.net32[lane - 16] = P.sub_cp32[16 * size_t(idx) + lane - 16];
-            __syncwarp();
-          }
-          if (lbc - rr >= best) continue;
-          if (kind == IK_FACE) {  // eval_item's analytic face, inline
-            if (S.cert[k] == 2) continue;  // no node's foot is within the trim
-            const DFace& f = P.faces[idx];
-            if (box_dist(p, f.box) >= best) continue;
-            double3 q, fn;
-            double u, v;
-            if (!analytic_foot(f, p, &q, &fn, &u, &v)) continue;
-            double d = len(p - q);
-            if (!(d < best) || (S.cert[k] != 1 && !trim_inside(P, f, u, v))) continue;
-            best = d;
-            sdv = d * sgn(dot(p - q, fn));
-            continue;
-          }
-          if (kind != IK_SUB) {
-            Acc A;
-            A.best = best;
-            A.sd = sdv;
-            A.und = INFINITY;
-            A.why = 0;
-            A.ub = INFINITY;
-            A.nd = 0;
-            A.record = true;  // an uncertified piece records its bound in und
-            eval_item_cold(P, code, p, A);
-            best = A.best;
-            sdv = A.sd;
-            if (A.und < INFINITY) defer_item(code, A.und);
-            continue;
-          }
-          const DSub& s = P.subs[idx];
-          double lb = box_dist(p, s.box);
-          if (lb >= best) continue;
-          if (!S.cert[k] && !sub_convex(s, p, p)) {
-            defer_item(code, lb);
-            continue;
-          }
-          int slot = S.slot[k];
-          double ss = 0.5, tt = 0.5;
-          if (slot >= 0) {
-            const Seed& sd = S.v.seed[slot];
-            double3 dp = p - c;
-            double gs = sd.ss[0] * dp.x + sd.ss[1] * dp.y + sd.ss[2] * dp.z;
-            double gt = sd.st[0] * dp.x + sd.st[1] * dp.y + sd.st[2] * dp.z;
-            ss = fmin(fmax(sd.s + sd.i00 * gs + sd.i01 * gt, 0.0), 1.0);
-            tt = fmin(fmax(sd.t + sd.i01 * gs + sd.i11 * gt, 0.0), 1.0);
-          }
-          const double4* cp64 = S.net;
-          bool conv;
-          if (MIXED) {
-            const float4* cp32 = S.net32;
-            float3 p32 = f3(float(p.x - s.c[0]), float(p.y - s.c[1]), float(p.z - s.c[2]));
-            float sf = float(ss), tf = float(tt);
-            newton_bicubic_f(cp32, p32, &sf, &tf, 8);
-            SEf ef = eval_bicubic_f(cp32, sf, tf);
-            float3 rf = f3(ef.p.x - p32.x, ef.p.y - p32.y, ef.p.z - p32.z);
-            double d32 = sqrt(double(dotf(rf, rf)));
-            // a float distance past the answer by more than its error cannot win
-            if (d32 > best + 1e-4 * (1.0 + best)) continue;
-            ss = sf, tt = tf;
-            newton_bicubic(cp64, p, &ss, &tt, 3, &conv);
-            if (!conv) newton_bicubic(cp64, p, &ss, &tt, 16, &conv);
-          } else {
-            newton_bicubic(cp64, p, &ss, &tt, 16, &conv);
-          }
-          if (!conv) {
-            defer_item(code, lb);
-            continue;
-          }
-          SE e = eval_bicubic(cp64, ss, tt);
-          double d = len(e.p - p);
-          if (!(d < best) || !is_critical(p, e)) continue;
-          double3 nrm = cross(e.ps, e.pt);
-          if (!(len(nrm) > 0.0)) continue;
-          if (s.klass != 1 &&
-              !trim_inside(P, P.faces[s.face], s.u0 + ss * (s.u1 - s.u0), s.v0 + tt * (s.v1 - s.v0)))
-            continue;
-          best = d;
-          sdv = d * sgn(dot(p - e.p, unit(nrm) * P.faces[s.face].sense));
-        }
-      }
-      if (!live) continue;
-      if (nd > 0 && nd <= 2 && und < best && und <= clamp)
-        node_resolve(P, p, dc0, dl0, dc1, dl1, nd, &best, &sdv, &und);
       double v;
       int f;
-      if (overflow || (und < best && und <= clamp)) {
-        node_fallback(P, p, clamp, &v, &f);
-      } else if (!isnan(sdv) && best <= clamp) {
-        v = sdv, f = 0;
-      } else {
-        v = clamp, f = 1;
-      }
+      warp_point<MIXED>(P, W, p, c, live, clamp, lane, &v, &f);
+      if (!live) continue;
       if (a.d_out) a.d_out[bi * 729 + nn] = v;
       if (a.flag_out) a.flag_out[bi * 729 + nn] = int8_t(f);
       S.flag[nn] = int8_t(f);

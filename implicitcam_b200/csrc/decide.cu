@@ -1,0 +1,160 @@
+// The box decision of a level (partcache.rs:226-331) on sm_100a: 32 boxes a warp, their
+// centres read through one shared candidate list, each box then decided air or material,
+// split, or (size 1) read.
+#include "kernels.h"
+#include "warp_list.cuh"
+
+namespace icam {
+
+constexpr int DWARPS = 4;  // box groups a block works on at once, one a warp
+
+struct DecideSmem {
+  uint32_t tcode[MAXC];  // the list before its ranking, and the walk's frontier
+  double tlb[MAXC];
+  int32_t fr[2][FR];
+  double lb[MAXC];  // ranked candidates
+  uint32_t code[MAXC];
+  Seed seed[MAXSUB];
+  double4 net[16];
+  float4 net32[16];
+  int8_t cert[MAXC];
+  int8_t slot[MAXC];
+  int n;
+};
+static_assert(sizeof(DecideSmem) * DWARPS <= 48 * 1024, "static shared memory of a block");
+
+// One box's verdict from its centre's value (v, f) read within `cut` (partcache.rs:370-383:
+// decided once the centre is known past the box grown by the clamp), the map entries it
+// settles, and its children (8 to a box, appended together) or its read.
+__device__ void decide_box(const DecideArgs& a, const Box4& b, double3 c, double r, double cut, double v, int f) {
+  const DPack& P = a.P;
+  const double side = 8.0 * a.h;
+  double sd = NAN;  // the signed distance at the centre when known
+  int verdict;      // 0 split or read, 1 air, 2 material
+  if (f == 0) {
+    sd = v;
+    verdict = (v - r > a.clamp) ? 1 : ((v + r < -a.clamp) ? 2 : 0);
+  } else if (f == 1) {
+    // past the box: air or material as the parent's centre when the parent's centre lies
+    // in this one's empty ball (partcache.rs:401-406); else read without the cut
+    if (isfinite(b.parent_sd) && b.parent_sd != 0.0 && b.reach < cut * (1.0 - 1e-6)) {
+      verdict = b.parent_sd > 0 ? 1 : 2;
+    } else {
+      point_fallback(P, c, INFINITY, &v, &f);
+      if (f == 0) {
+        sd = v;
+        verdict = (v - r > a.clamp) ? 1 : ((v + r < -a.clamp) ? 2 : 0);
+      } else {
+        verdict = 0;
+      }
+    }
+  } else {
+    verdict = 0;
+  }
+  const long long nb0 = a.nb[0], nb1 = a.nb[1], nb2 = a.nb[2];
+  if (verdict != 0) {
+    uint32_t val = verdict == 1 ? 0xffffffffu : 0xfffffffeu;
+    for (long long z = max(b.z, 0LL); z < min(b.z + a.size, nb2); z++)
+      for (long long y = max(b.y, 0LL); y < min(b.y + a.size, nb1); y++)
+        for (long long x = max(b.x, 0LL); x < min(b.x + a.size, nb0); x++) a.map[x + nb0 * (y + nb1 * z)] = val;
+  } else if (a.size == 1) {
+    long long idx = b.x + nb0 * (b.y + nb1 * b.z);
+    a.map[idx] = 0xfffffff0u;  // read
+    unsigned long long slot = atomicAdd(a.n_read, 1ull);
+    if (slot < (unsigned long long)a.read_cap) {
+      a.read_idx[slot] = idx;
+      a.read_dc[slot] = sd;
+    }
+  } else {
+    const long long half = a.size / 2;
+    Box4 kids[8];
+    int nk = 0;
+    for (int q = 0; q < 8; q++) {
+      Box4 k;
+      k.x = b.x + half * (q & 1);
+      k.y = b.y + half * ((q >> 1) & 1);
+      k.z = b.z + half * ((q >> 2) & 1);
+      if (!(k.x < nb0 && k.x + half > 0 && k.y < nb1 && k.y + half > 0 && k.z < nb2 && k.z + half > 0)) continue;
+      double3 klo = mk(a.lo[0] + side * k.x - a.clamp, a.lo[1] + side * k.y - a.clamp, a.lo[2] + side * k.z - a.clamp);
+      double3 khi = mk(a.lo[0] + side * (k.x + half) + a.clamp, a.lo[1] + side * (k.y + half) + a.clamp,
+                       a.lo[2] + side * (k.z + half) + a.clamp);
+      k.reach = len((klo + khi) * 0.5 - c);
+      k.parent_sd = sd;
+      kids[nk++] = k;
+    }
+    // together, so that the next level's warps take neighbouring boxes
+    unsigned long long slot = atomicAdd(a.n_next, (unsigned long long)nk);
+    for (int q = 0; q < nk; q++)
+      if (slot + q < (unsigned long long)a.next_cap) a.next[slot + q] = kids[q];
+  }
+}
+
+// 32 boxes a warp: their centres' bounding ball, the features within its radius plus the
+// cut of its centre (listed and ranked once, sub-patches seeded there), every centre's
+// value capped at the cut by the shared walk, then each box decided.
+__global__ void __launch_bounds__(DWARPS * 32, 2) k_decide_w(DecideArgs a) {
+  __shared__ DecideSmem smem[DWARPS];
+  const DPack& P = a.P;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  DecideSmem& S = smem[warp];
+  const double side = 8.0 * a.h;
+  for (int64_t g0 = (int64_t(blockIdx.x) * DWARPS + warp) * 32; g0 < a.n; g0 += int64_t(gridDim.x) * DWARPS * 32) {
+    const int64_t i = g0 + lane;
+    const bool live = i < a.n;
+    const Box4 b = a.boxes[live ? i : g0];
+    double3 lo = mk(a.lo[0] + side * b.x - a.clamp, a.lo[1] + side * b.y - a.clamp, a.lo[2] + side * b.z - a.clamp);
+    double3 hi = mk(a.lo[0] + side * (b.x + a.size) + a.clamp, a.lo[1] + side * (b.y + a.size) + a.clamp,
+                    a.lo[2] + side * (b.z + a.size) + a.clamp);
+    const double3 c = (lo + hi) * 0.5;
+    const double r = 0.5 * len(hi - lo);
+    const double cut = (r + a.clamp) * (1.0 + 1e-4);
+    // the group's centre: the middle of its centres' box; its radius, the farthest centre
+    double bl[3] = {c.x, c.y, c.z}, bh[3] = {c.x, c.y, c.z};
+    for (int o = 16; o > 0; o >>= 1)
+      for (int k = 0; k < 3; k++) {
+        bl[k] = fmin(bl[k], __shfl_xor_sync(FULL, bl[k], o));
+        bh[k] = fmax(bh[k], __shfl_xor_sync(FULL, bh[k], o));
+      }
+    const double3 gc = mk(0.5 * (bl[0] + bh[0]), 0.5 * (bl[1] + bh[1]), 0.5 * (bl[2] + bh[2]));
+    double R = len(c - gc);
+    for (int o = 16; o > 0; o >>= 1) R = fmax(R, __shfl_xor_sync(FULL, R, o));
+    // every feature nearer than the cut to a centre has a bound <= R + cut from gc
+    int n = warp_list(P, a.leaves, a.n_leaves, gc, R + cut, S.tcode, S.tlb, S.fr, &S.n, lane);
+    const bool overflow = n > MAXC;
+    if (overflow) n = MAXC;
+    warp_rank(S.tcode, S.tlb, n, S.code, S.lb, lane);
+    int subs_before = 0;
+    for (int base = 0; base < n; base += 32) {
+      const int k = base + lane;
+      const bool is_sub = k < n && (S.code[k] >> IK_SHIFT) == IK_SUB;
+      const unsigned m = __ballot_sync(FULL, is_sub);
+      const int before = subs_before + __popc(m & ((1u << lane) - 1u));
+      subs_before += __popc(m);
+      if (k >= n) continue;
+      int slot = -1;
+      if (is_sub && before < MAXSUB) {
+        slot = before;
+        S.seed[slot] = seed_at(P.sub_cp + 16 * size_t(S.code[k] & IK_MASK), gc);
+      }
+      S.cert[k] = 0;
+      S.slot[k] = int8_t(slot);
+    }
+    __syncwarp();
+    const WarpCands W{S.code, S.lb, S.cert, S.slot, S.seed, S.net, S.net32, n, overflow};
+    double v;
+    int f;
+    warp_point<false>(P, W, c, gc, live, cut, lane, &v, &f);
+    if (live) decide_box(a, b, c, r, cut, v, f);
+    __syncwarp();
+  }
+}
+
+void launch_decide(const DecideArgs& a, cudaStream_t s) {
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int64_t want = (a.n + DWARPS * 32 - 1) / (DWARPS * 32);
+  const int grid = int(std::max<int64_t>(1, std::min<int64_t>(want, int64_t(sms) * 2)));
+  k_decide_w<<<grid, DWARPS * 32, 0, s>>>(a);
+}
+
+}  // namespace icam

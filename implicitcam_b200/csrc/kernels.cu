@@ -1,6 +1,6 @@
-// Kernels of the exact part field on sm_100a besides the brick kernel (bricks.cu): point
-// queries through the feature tree, the box decision of a level (partcache.rs:226-331),
-// the gather of the read bricks and the assembly of the map and the atlas.
+// Kernels of the exact part field on sm_100a besides the brick kernel (bricks.cu) and the
+// box decision (decide.cu): point queries through the feature tree, the gather of the
+// read bricks and the assembly of the map and the atlas.
 #include "field.cuh"
 #include "kernels.h"
 
@@ -19,85 +19,6 @@ __global__ void k_points(DPack P, const double* __restrict__ xyz, int64_t n, dou
     finish(A, cap, &v, &f);
     value[i] = v;
     flag[i] = int8_t(f);
-  }
-}
-
-// ---------------------------------------------------------------- the decision of a level
-
-// One box of bricks [first, first + size) a thread: its centre read within `cut`
-// (partcache.rs:370-383: a box is decided once its centre is known past the box grown by
-// the clamp), decided air or material, split, or (size 1) read.
-__global__ void k_decide(DecideArgs a) {
-  const DPack& P = a.P;
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < a.n; i += int64_t(gridDim.x) * blockDim.x) {
-    Box4 b = a.boxes[i];
-    double side = 8.0 * a.h;
-    double3 lo = mk(a.lo[0] + side * b.x - a.clamp, a.lo[1] + side * b.y - a.clamp, a.lo[2] + side * b.z - a.clamp);
-    double3 hi = mk(a.lo[0] + side * (b.x + a.size) + a.clamp, a.lo[1] + side * (b.y + a.size) + a.clamp,
-                    a.lo[2] + side * (b.z + a.size) + a.clamp);
-    double3 c = (lo + hi) * 0.5;
-    double r = 0.5 * len(hi - lo);
-    double cut = (r + a.clamp) * (1.0 + 1e-4);
-    Acc A;
-    point_query(P, c, cut, A);
-    double v;
-    int f;
-    finish(A, cut, &v, &f);
-    double sd = NAN;  // the signed distance at the centre when known
-    int verdict;      // 0 split or read, 1 air, 2 material
-    if (f == 0) {
-      sd = v;
-      verdict = (v - r > a.clamp) ? 1 : ((v + r < -a.clamp) ? 2 : 0);
-    } else if (f == 1) {
-      // past the box: air or material as the parent's centre when the parent's centre
-      // lies in this one's empty ball (partcache.rs:401-406); else read without the cut
-      double reach = b.reach;
-      if (isfinite(b.parent_sd) && b.parent_sd != 0.0 && reach < cut * (1.0 - 1e-6)) {
-        verdict = b.parent_sd > 0 ? 1 : 2;
-      } else {
-        point_query(P, c, INFINITY, A);
-        finish(A, INFINITY, &v, &f);
-        if (f == 0) {
-          sd = v;
-          verdict = (v - r > a.clamp) ? 1 : ((v + r < -a.clamp) ? 2 : 0);
-        } else {
-          verdict = 0;
-        }
-      }
-    } else {
-      verdict = 0;
-    }
-    long long nb0 = a.nb[0], nb1 = a.nb[1], nb2 = a.nb[2];
-    if (verdict != 0) {
-      uint32_t val = verdict == 1 ? 0xffffffffu : 0xfffffffeu;
-      for (long long z = max(b.z, 0LL); z < min(b.z + a.size, nb2); z++)
-        for (long long y = max(b.y, 0LL); y < min(b.y + a.size, nb1); y++)
-          for (long long x = max(b.x, 0LL); x < min(b.x + a.size, nb0); x++) a.map[x + nb0 * (y + nb1 * z)] = val;
-    } else if (a.size == 1) {
-      long long idx = b.x + nb0 * (b.y + nb1 * b.z);
-      a.map[idx] = 0xfffffff0u;  // read
-      unsigned long long slot = atomicAdd((unsigned long long*)a.n_read, 1ull);
-      if (slot < (unsigned long long)a.read_cap) {
-        a.read_idx[slot] = idx;
-        a.read_dc[slot] = sd;
-      }
-    } else {
-      long long half = a.size / 2;
-      for (int q = 0; q < 8; q++) {
-        Box4 k;
-        k.x = b.x + half * (q & 1);
-        k.y = b.y + half * ((q >> 1) & 1);
-        k.z = b.z + half * ((q >> 2) & 1);
-        if (!(k.x < nb0 && k.x + half > 0 && k.y < nb1 && k.y + half > 0 && k.z < nb2 && k.z + half > 0)) continue;
-        double3 klo = mk(a.lo[0] + side * k.x - a.clamp, a.lo[1] + side * k.y - a.clamp, a.lo[2] + side * k.z - a.clamp);
-        double3 khi = mk(a.lo[0] + side * (k.x + half) + a.clamp, a.lo[1] + side * (k.y + half) + a.clamp,
-                         a.lo[2] + side * (k.z + half) + a.clamp);
-        k.reach = len((klo + khi) * 0.5 - c);
-        k.parent_sd = sd;
-        unsigned long long slot = atomicAdd((unsigned long long*)a.n_next, 1ull);
-        if (slot < (unsigned long long)a.next_cap) a.next[slot] = k;
-      }
-    }
   }
 }
 

@@ -38,6 +38,8 @@ struct BrickArgs {
 
 struct DecideArgs {
   DPack P;
+  const int32_t* leaves;  // the tree's leaf nodes
+  int32_t n_leaves;
   const Box4* boxes;
   int64_t n;
   long long size;
@@ -59,7 +61,8 @@ __global__ void k_points(DPack P, const double* xyz, int64_t n, double cap, doub
 // The brick kernel (bricks.cu) in the arithmetic a.mixed names, one warp a brick over a
 // grid sized for the current device.
 void launch_bricks(const BrickArgs& a, cudaStream_t s);
-__global__ void k_decide(DecideArgs a);
+// The decision of one box size of a level (decide.cu), 32 boxes a warp.
+void launch_decide(const DecideArgs& a, cudaStream_t s);
 __global__ void k_gather_firsts(const int64_t* idx, int64_t n, int64_t nb0, int64_t nb1, double h, double lo0,
                                 double lo1, double lo2, double* firsts);
 __global__ void k_assemble(const int64_t* idx, const int32_t* kind, const int64_t* slot, int64_t n,
