@@ -455,10 +455,12 @@ HD SEf eval_bicubic_f(const float4* cp, float s, float t) {
 
 // The projected Newton of newton_bicubic in floats (rebased point p), to a step under
 // 1e-6 of the square; the double polish takes it from there.
-HDI void newton_bicubic_f(const float4* cp, float3 p, float* ps_, float* pt_, int iters) {
+// *last: the patch at the point of the last step's start (within that step of the end).
+HDI void newton_bicubic_f(const float4* cp, float3 p, float* ps_, float* pt_, int iters, SEf* last) {
   float s = *ps_, t = *pt_;
   for (int it = 0; it < iters; it++) {
     SEf e = eval_bicubic_f(cp, s, t);
+    *last = e;
     float3 r = f3(e.p.x - p.x, e.p.y - p.y, e.p.z - p.z);
     float g0 = dotf(e.ps, r), g1 = dotf(e.pt, r);
     float jss = dotf(e.ps, e.ps), jst = dotf(e.ps, e.pt), jtt = dotf(e.pt, e.pt);

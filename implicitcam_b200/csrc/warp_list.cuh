@@ -279,8 +279,8 @@ __device__ __forceinline__ void warp_point(const DPack& P, const WarpCands& W, d
       const float4* cp32 = W.net32;
       float3 p32 = f3(float(p.x - s.c[0]), float(p.y - s.c[1]), float(p.z - s.c[2]));
       float sf = float(ss), tf = float(tt);
-      newton_bicubic_f(cp32, p32, &sf, &tf, 8);
-      SEf ef = eval_bicubic_f(cp32, sf, tf);
+      SEf ef;
+      newton_bicubic_f(cp32, p32, &sf, &tf, 8, &ef);
       float3 rf = f3(ef.p.x - p32.x, ef.p.y - p32.y, ef.p.z - p32.z);
       double d32 = sqrt(double(dotf(rf, rf)));
       // a float distance past the answer by more than its error cannot win
