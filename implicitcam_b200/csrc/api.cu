@@ -15,28 +15,9 @@
 #include "../../include/icam_cuda.h"
 #include "kernels.h"
 #include "pack_build.h"
+#include "pack_state.h"
 
 using namespace icam;
-
-struct IcamPack {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  HostPack host;
-  DPack dev{};
-  std::vector<void*> owned;  // the pack's device arrays
-  std::vector<int32_t> leaves_host;
-  int32_t* leaves = nullptr;
-  // scratch, grown on demand
-  struct Buf {
-    void* p = nullptr;
-    size_t n = 0;
-  };
-  Buf scratch[16];
-  std::string err;
-  unsigned long long* d_stats = nullptr;
-  const uint32_t* last_map = nullptr;
-  const uint32_t* last_atlas = nullptr;
-};
 
 namespace {
 

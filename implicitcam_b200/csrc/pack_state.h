@@ -1,0 +1,51 @@
+// What an IcamPack holds (include/icam_cuda.h keeps it opaque): the packed solid on the
+// device, its stream, scratch grown on demand, and the seed network's state.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "pack_build.h"
+
+// The learned seeds (seednet.cu): per sub-patch features, the network's FP32 master
+// weights and Adam moments for training, the BF16 copy the kernels read, and the
+// training batch. All device arrays, allocated on first use and kept in `owned`.
+struct SeedNetState {
+  float* feat = nullptr;    // SN_FEAT floats a sub-patch
+  float* params = nullptr;  // SN_PARAMS, FP32 master
+  float* grads = nullptr;
+  float* adam_m = nullptr;
+  float* adam_v = nullptr;
+  void* wbf = nullptr;      // BF16 transposed weights (SN_TBF) then FP32 biases
+  float* x = nullptr;       // batch inputs (SN_INP a sample) and targets (4 a sample)
+  float* y = nullptr;
+  int64_t batch_cap = 0;
+  unsigned long long* step = nullptr;  // the step the device-side training is on
+  float* loss = nullptr;               // loss per step
+  int64_t loss_cap = 0;
+  bool ready = false;       // weights set (trained or loaded)
+};
+
+struct IcamPack {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  icam::HostPack host;
+  icam::DPack dev{};
+  std::vector<void*> owned;  // the pack's device arrays
+  std::vector<int32_t> leaves_host;
+  int32_t* leaves = nullptr;
+  // scratch, grown on demand
+  struct Buf {
+    void* p = nullptr;
+    size_t n = 0;
+  };
+  Buf scratch[16];
+  std::string err;
+  unsigned long long* d_stats = nullptr;
+  const uint32_t* last_map = nullptr;
+  const uint32_t* last_atlas = nullptr;
+  SeedNetState net;
+};

@@ -67,6 +67,12 @@ def lib():
         L.icam_pack_stream.restype = vp
         L.icam_pack_stream.argtypes = [vp]
         L.icam_probe_fma.argtypes = [vp, C.c_int, C.POINTER(C.c_double)]
+        u64, d = C.c_uint64, C.c_double
+        L.icam_seednet_samples.argtypes = [vp, sz, u64, d, vp, vp]
+        L.icam_seednet_params.argtypes = [vp, vp, vp, C.POINTER(sz)]
+        L.icam_seednet_grad.argtypes = [vp, vp, vp, sz, vp, C.POINTER(d)]
+        L.icam_seednet_train.argtypes = [vp, C.c_int64, C.c_int64, u64, d, d, vp]
+        L.icam_seednet_ab.argtypes = [vp, sz, u64, d, vp]
         _lib = L
     return _lib
 
@@ -207,6 +213,49 @@ class PartGpu:
 
     def warm(self, secs):
         self._check(lib().icam_warm(self.h, float(secs)), "icam_warm")
+
+    # ---- the seed network (no counterpart in the reference; see include/icam_cuda.h)
+
+    def seednet_samples(self, n, seed=0, need=2.0):
+        """n training pairs from the exact evaluator: inputs (n x 32) and targets
+        (n x 4: s, t, d / L, 1)."""
+        x = np.zeros((n, 32), np.float32)
+        y = np.zeros((n, 4), np.float32)
+        self._check(lib().icam_seednet_samples(self.h, n, seed, float(need), _p(x), _p(y)), "icam_seednet_samples")
+        return x, y
+
+    def seednet_params(self, set_to=None):
+        """The FP32 parameter vector (after setting it to `set_to` when given)."""
+        n = C.c_size_t()
+        lib().icam_seednet_params(self.h, None, None, C.byref(n))
+        out = np.zeros(n.value, np.float32)
+        src = None if set_to is None else np.ascontiguousarray(set_to, dtype=np.float32)
+        self._check(lib().icam_seednet_params(self.h, _p(out), _p(src), C.byref(n)), "icam_seednet_params")
+        return out
+
+    def seednet_grad(self, x, y):
+        """Gradient of the mean loss over pairs (x, y) at the current parameters, and the loss."""
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.ascontiguousarray(y, dtype=np.float32)
+        g = np.zeros(len(self.seednet_params()), np.float32)
+        loss = C.c_double()
+        self._check(lib().icam_seednet_grad(self.h, _p(x), _p(y), len(x), _p(g), C.byref(loss)), "icam_seednet_grad")
+        return g, loss.value
+
+    def seednet_train(self, steps, batch=4096, seed=0, need=2.0, lr=1e-3):
+        """Trains on fresh pairs; the loss of every step."""
+        loss = np.zeros(max(steps, 1), np.float32)
+        self._check(lib().icam_seednet_train(self.h, steps, batch, seed, float(need), float(lr), _p(loss)),
+                    "icam_seednet_train")
+        return loss[:steps]
+
+    def seednet_ab(self, n, seed=1, need=2.0):
+        """The net's Newton starts against the centre start on n fresh pairs."""
+        st = np.zeros(8)
+        self._check(lib().icam_seednet_ab(self.h, n, seed, float(need), _p(st)), "icam_seednet_ab")
+        keys = ["pairs", "mean_iters_net", "mean_iters_centre", "p99_iters_net", "p99_iters_centre",
+                "fallback_rate", "pairs_differing", "max_diff_over_L"]
+        return dict(zip(keys, st.tolist()))
 
 
 def unpack_atlas(atlas):

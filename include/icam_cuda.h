@@ -164,6 +164,40 @@ void* icam_pack_stream(const IcamPack* pack);
 /* The last error message of a call on this pack. */
 const char* icam_last_error(const IcamPack* pack);
 
+/* ---- The seed network (ICAM_MIXED_LEARNED). No counterpart in the reference, which
+ * starts every Newton solve on a B-spline sub-patch at its centre: a small MLP
+ * (query in the sub-patch's frame + a 16-number descriptor -> 64 -> 64 -> 64 ->
+ * (s, t, distance / L)) predicts the start; each start is checked by the solve it
+ * starts (convergence and the critical-point test), with the centre start as the
+ * fallback, so the answers stay the exact evaluator's. Trained on the device by the
+ * library's own kernels on pairs the exact FP64 evaluator makes; run on the tensor
+ * cores in BF16. Weights live in the pack; the parameter vector's layout is
+ * W1[32][64] b1[64] W2[64][64] b2[64] W3[64][64] b3[64] W4[64][8] b4[8] (row = input,
+ * column = output; inputs past 19 and outputs past 3 are padding). */
+
+/* n training pairs from the exact evaluator (sub-patch points moved along the normal
+ * by up to `need` and across the patch): x_out n x 32 inputs (19 used), y_out n x 4
+ * targets (s, t, d / L, 1). */
+int icam_seednet_samples(IcamPack* pack, size_t n, uint64_t seed, double need, float* x_out, float* y_out);
+
+/* Reads (get) and/or sets (set) the FP32 parameters; *n_params their count. */
+int icam_seednet_params(IcamPack* pack, float* get, const float* set, size_t* n_params);
+
+/* The gradient of the mean loss (s - s*)^2 + (t - t*)^2 + 0.1 (d - d*)^2 over the n
+ * pairs (x n x 32, y n x 4) at the current parameters, and that loss. */
+int icam_seednet_grad(IcamPack* pack, const float* x, const float* y, size_t n, float* grad_out, double* loss_out);
+
+/* Trains for `steps` Adam steps of `batch` fresh pairs each (one CUDA graph replayed);
+ * loss_out (optional, steps floats) the loss of every step. */
+int icam_seednet_train(IcamPack* pack, int64_t steps, int64_t batch, uint64_t seed, double need, double lr,
+                       float* loss_out);
+
+/* The net's starts against the centre start on n fresh pairs: stats[0] pairs, [1] mean
+ * Newton iterations from the net, [2] from the centre, [3] and [4] their 99th
+ * percentiles, [5] the fallback rate, [6] pairs whose answers differ by more than
+ * 1e-9 of the sub-patch's size, [7] the largest such difference over that size. */
+int icam_seednet_ab(IcamPack* pack, size_t n, uint64_t seed, double need, double stats[8]);
+
 #ifdef __cplusplus
 }
 #endif
