@@ -10,7 +10,11 @@ surface exact, the rest clamped), over the part's box grown by the band. A voxel
 a cell of a brick the bake reads (512 a brick). Under torchrun each rank bakes its
 own part (seed = rank): weak scaling, no collective on the data path.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed|learned]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision learned|mixed|fp64]
+
+The headline arm (default: mixed precision with the seed network's Newton starts) is
+timed beside the plain FP64 kernel on the same level; the line carries both, the
+speed-up, and the headline's error against FP64 (map, signs, i16 words, distances).
     python bench.py --impl reference ...   # the reference's CPU path (the oracle port)
 
 Prints one JSON line (rank 0).
@@ -38,6 +42,8 @@ BAND = 2.0
 # B-spline span, line or arc edge, spline edge piece, vertex): foot + uv + one parity
 # leg; 6 Newton steps of 750 + trim 200; closed-form foot; 6 steps of 120; a distance
 FLOPS_PER_CANDIDATE = np.array([80.0, 6 * 750.0 + 200.0, 40.0, 6 * 120.0, 10.0])
+# the seed network's training: 50M pairs from the exact evaluator, before any timing
+SEEDNET_STEPS, SEEDNET_BATCH = 12208, 4096
 
 
 def set_level(h, band):
@@ -152,7 +158,8 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed", "learned"])
+    ap.add_argument("--precision", default="learned", choices=["fp64", "mixed", "learned"],
+                    help="the headline arm; the plain FP64 arm is timed beside it")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--h", type=float, default=H, help="cell side (mm); smaller cases for profiling")
     ap.add_argument("--band", type=float, default=BAND, help="narrow band half-width (mm), the clamp")
@@ -182,54 +189,72 @@ def main():
     g = part_gpu.PartGpu(b, need=need, device=local)
     stream = torch.cuda.ExternalStream(g.stream(), device=local)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")  # > L2 (126 MB)
+    seednet = None
+    if prec == part_gpu.MIXED_LEARNED:  # trained before any timing: 50M pairs from the exact evaluator
+        t0 = time.perf_counter()
+        loss = g.seednet_train(SEEDNET_STEPS, batch=SEEDNET_BATCH, seed=rank, need=need)
+        torch.cuda.synchronize()
+        seednet = {"train_pairs": SEEDNET_STEPS * SEEDNET_BATCH, "train_s": time.perf_counter() - t0,
+                   "final_loss": float(loss[-50:].mean()), "ab": g.seednet_ab(1 << 20, seed=rank + 7, need=need)}
 
-    def step(device_only=True, host=None):
+    def step(p, device_only=True, host=None):
         flush.zero_()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         if device_only:
-            _, _, ns, st = g.level_device(H, lo, nb, BAND, precision=prec)
+            _, _, ns, st = g.level_device(H, lo, nb, BAND, precision=p)
         else:
             m, a = host
-            ns, st = g.level_into(H, lo, nb, BAND, m, a, precision=prec)
+            ns, st = g.level_into(H, lo, nb, BAND, m, a, precision=p)
         e1.record(stream)
         e1.synchronize()
         return e0.elapsed_time(e1), ns, st
 
-    for _ in range(args.warmup):
-        step()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
+    def arm(p):
+        """W warm-up steps, then K timed steps between barriers: (ms max over ranks,
+        voxels over ranks, stats of each step)."""
+        for _ in range(args.warmup):
+            step(p)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ms, stats = [], []
+        for _ in range(args.steps):
+            t, ns, st = step(p)
+            ms.append(t)
+            stats.append(st)
+        torch.cuda.synchronize()
+        total_ms, voxels = float(sum(ms)), 512.0 * stats[-1]["bricks_read"]
+        if dist:
+            t = torch.tensor([total_ms], device=f"cuda:{local}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            total_ms = float(t.item())
+            v = torch.tensor([voxels], device=f"cuda:{local}", dtype=torch.float64)
+            dist.all_reduce(v)
+            voxels = float(v.item())
+            dist.barrier()
+        return total_ms, voxels, stats
+
     clk_path = os.path.join(tempfile.gettempdir(), f"icam_clocks_{os.getpid()}.csv")
     smi = sample_clocks(clk_path) if rank == 0 else None
-    ms, stats = [], []
-    for _ in range(args.steps):
-        t, ns, st = step()
-        ms.append(t)
-        stats.append(st)
-    torch.cuda.synchronize()
+    total_ms, voxels, stats = arm(prec)
+    fp64 = None
+    if prec != part_gpu.FP64:
+        f_ms, f_vox, f_stats = arm(part_gpu.FP64)
+        fp64 = {"value": f_vox * args.steps / (f_ms * 1e-3), "ms_per_step": f_ms / args.steps,
+                "stage_ms": {"decide": f_stats[-1]["ms_decide"], "nodes": f_stats[-1]["ms_nodes"],
+                             "assemble": f_stats[-1]["ms_post"]}}
     if smi:
         smi.terminate()
         smi.wait()
-    total_ms = float(sum(ms))
-    voxels = 512.0 * stats[-1]["bricks_read"]
-    if dist:
-        t = torch.tensor([total_ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-        v = torch.tensor([voxels], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(v)
-        voxels = float(v.item())
-        dist.barrier()
     value = voxels * args.steps / (total_ms * 1e-3)
     # end to end through the C ABI: the map and atlas read back into pinned host memory
     m_host = torch.empty(int(np.prod(nb)), dtype=torch.int32, pin_memory=True)
     a_host = torch.empty((max(stats[-1]["bricks_words"], 1) * part_gpu.WORDS,), dtype=torch.int32, pin_memory=True)
     e2e_ms = []
     for _ in range(max(1, args.steps)):
-        t, ns, st = step(device_only=False, host=(m_host, a_host))
+        t, ns, st = step(prec, device_only=False, host=(m_host, a_host))
         e2e_ms.append(t)
     e2e_total = float(sum(e2e_ms))
     if dist:
@@ -238,6 +263,9 @@ def main():
         e2e_total = float(t.item())
     e2e_value = voxels * len(e2e_ms) / (e2e_total * 1e-3)
     d2h = int(np.prod(nb)) * 4 + stats[-1]["bricks_words"] * part_gpu.WORDS * 4
+    error = None
+    if fp64 is not None:
+        error = compare_with_fp64(g, part_gpu, prec, lo, nb, m_host.numpy().copy(), a_host.numpy().copy())
     if rank == 0:
         st = stats[-1]
         node_ms = float(np.mean([s["ms_nodes"] for s in stats]))
@@ -258,6 +286,8 @@ def main():
             "config": {"workload": f"freeform-top level bake, h={H} mm, band +-{BAND} mm", "part": "freeform_top",
                        "seed": "rank", "h_mm": H, "band_mm": BAND, "nb": nb.tolist(), "precision": args.precision,
                        "l2": "flushed (256 MB write) before every step"},
+            "speedup_vs_fp64": None if fp64 is None else value / fp64["value"],
+            "fp64": fp64, "error_vs_fp64": error, "seednet": seednet,
             "bricks_read": st["bricks_read"], "bricks_stored": st["bricks_words"],
             "nodes_exact": st["nodes_exact"], "nodes_undecided": st["nodes_undecided"],
             "stage_ms": {"decide": st["ms_decide"], "nodes": st["ms_nodes"], "assemble": st["ms_post"]},
@@ -276,6 +306,31 @@ def main():
     g.close()
     if dist:
         dist.destroy_process_group()
+
+
+def compare_with_fp64(g, part_gpu, prec, lo, nb, m_arm, a_arm):
+    """The headline arm's level against the plain FP64 kernel's: the map (active set and
+    AIR / SOLID signs) equal, the i16 words' largest difference and sign flips, and the
+    largest distance difference over the diagonal on a sample of stored bricks."""
+    m64, a64, _ = g.level(H, lo, nb, BAND, precision=part_gpu.FP64)
+    m_arm = m_arm.view(np.uint32)[: len(m64)]
+    same_map = bool((m_arm == m64).all())
+    q64 = part_gpu.unpack_atlas(a64).astype(np.int64)
+    qa = part_gpu.unpack_atlas(a_arm.view(np.uint32)[: a64.size]).astype(np.int64)
+    flips = int(((q64 > 0) & (qa < 0)).sum() + ((q64 < 0) & (qa > 0)).sum())
+    stored = np.nonzero(m64 < 0xFFFFFFF0)[0]
+    rng = np.random.default_rng(0)
+    pick = stored[rng.permutation(len(stored))[:256]]
+    idx = np.stack([pick % nb[0], (pick // nb[0]) % nb[1], pick // (nb[0] * nb[1])], 1)
+    firsts = lo + 8 * H * idx
+    _, d64 = g.bricks(firsts, H, BAND, precision=part_gpu.FP64)
+    _, da = g.bricks(firsts, H, BAND, precision=prec)
+    diag = float(np.linalg.norm(np.asarray(nb) * 8 * H - 2 * BAND))  # the part's box, about
+    ok = (np.abs(d64) < BAND) & (np.abs(da) < BAND)
+    return {"map_equal": same_map, "i16_max_step_diff": int(np.abs(q64 - qa).max()) if q64.size else 0,
+            "sign_flips": flips, "max_abs_mm": float(np.abs(d64 - da)[ok].max()) if ok.any() else 0.0,
+            "max_over_diag": float(np.abs(d64 - da)[ok].max() / diag) if ok.any() else 0.0,
+            "sample": f"{len(pick)} stored bricks, every node within the band"}
 
 
 if __name__ == "__main__":

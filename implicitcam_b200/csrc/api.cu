@@ -61,6 +61,17 @@ int scratch(IcamPack* pk, int k, size_t bytes, void** out) {
   return ICAM_OK;
 }
 
+// ICAM_MIXED_LEARNED: the seed network's starts for the brick kernel (it must have been
+// trained or loaded on this pack).
+int learned_starts(IcamPack* pk, int precision, BrickArgs* a) {
+  if (precision != ICAM_MIXED_LEARNED) return ICAM_OK;
+  if (!pk->net.ready)
+    return fail(pk, ICAM_ERR_ARG, "ICAM_MIXED_LEARNED: train (icam_seednet_train) or load the seed network first");
+  a->net_feat = pk->net.feat;
+  a->net_w = pk->net.wbf;
+  return ICAM_OK;
+}
+
 int grid_for(int64_t n, int threads) {
   int64_t g = (n + threads - 1) / threads;
   return int(std::max<int64_t>(1, std::min<int64_t>(g, 148 * 32)));
@@ -225,6 +236,7 @@ int icam_bricks(IcamPack* pk, const double* first_nodes, size_t n, double h, dou
   a.leaves = pk->leaves;
   a.n_leaves = int32_t(pk->leaves_host.size());
   a.mixed = precision != ICAM_FP64;
+  if ((r = learned_starts(pk, precision, &a))) return r;
   a.d_out = (double*)dval;
   a.flag_out = (int8_t*)dflag;
   a.stats = pk->d_stats;
@@ -364,6 +376,7 @@ static int bake_level(IcamPack* pk, double h, const double lo[3], const int64_t 
     b.leaves = pk->leaves;
     b.n_leaves = int32_t(pk->leaves_host.size());
     b.mixed = precision != ICAM_FP64;
+    if ((r = learned_starts(pk, precision, &b))) return r;
     b.words_out = (uint32_t*)d_words;
     b.kind_out = (int32_t*)d_kind;
     b.stats = pk->d_stats;

@@ -4,6 +4,7 @@
 #include <type_traits>
 
 #include "kernels.h"
+#include "seednet.cuh"
 #include "warp_list.cuh"
 
 namespace icam {
@@ -21,7 +22,6 @@ __device__ __forceinline__ int nb_of(int n, int k, double* dist) {
   *dist = sqrt(double(di * di + dj * dj + dk * dk));
   return a + 9 * b + 81 * c;
 }
-
 
 // A warp's shared memory for its brick. The list before its ranking and the walk's
 // frontier share room with the node values, which come later.
@@ -51,6 +51,7 @@ struct BrickSmem {
   int n;
 };
 static_assert(sizeof(BrickSmem) * WARPS <= 48 * 1024, "static shared memory of a block");
+static_assert(sizeof(((BrickSmem*)0)->u) >= 32 * SN_KS * 2 + 32 * 8 * 4, "the seed network's room in the list's");
 
 __device__ __forceinline__ uint32_t spread(uint32_t m) { return m | (m << 1) | (m >> 1); }
 
@@ -116,17 +117,15 @@ __device__ void flood(BrickSmem& S, int lane) {
 //     sqrt(3) + clamp of the brick's centre giving its features within that bound
 //     (GpuPack::list with r = 0, partcache.rs:767), ranked by the bound;
 //  2. each of the first MAXSUB sub-patches: its convexity certified for the whole brick
-//     and its Newton solution at the centre kept for seeds, a lane each;
-//  3. 23 passes of 32 nodes: candidate by candidate, every lane on its node at once (the
-//     warp leaves when all its nodes are nearer than the next bound), each node capped at
-//     the clamp; a feature uncertified at a node sends that node to the tree walk;
+//     and its Newton solution at the centre kept for seeds, a lane each (started where
+//     the seed network puts it when one is given); each plane's trim classified over
+//     the feet of the whole brick;
+//  3. 23 passes of 32 nodes, each node's value by the warp's shared candidate walk
+//     (warp_point, warp_list.cuh), capped at the clamp;
 //  4. far nodes signed, undecided ones bridged, quantised and packed.
-// MIXED: sub-patches run Newton in floats on the rebased nets and are polished in
-// doubles (with the critical-point test and the trim) only when their float distance
-// can beat the node's answer.
-template <bool MIXED>
 // Two blocks a SM: the evaluators' register need (255 a thread) left unspilled beats
 // more warps with spills (measured: 8 warps a SM 240 ms, 16 warps 280 ms a bake).
+template <bool MIXED>
 __global__ void __launch_bounds__(WARPS * 32, 2) k_bricks_t(BrickArgs a) {
   __shared__ BrickSmem smem[WARPS];
   const DPack& P = a.P;
@@ -180,6 +179,18 @@ __global__ void __launch_bounds__(WARPS * 32, 2) k_bricks_t(BrickArgs a) {
         const unsigned m = __ballot_sync(FULL, is_sub);
         const int before = subs_before + __popc(m & ((1u << lane) - 1u));
         subs_before += __popc(m);
+        // MIXED_LEARNED: the centre solves start where the seed network puts them, its 32
+        // queries (this group of candidates at the centre) on the tensor cores, in the
+        // room of the list, which is ranked by now
+        double s0 = 0.5, t0 = 0.5;
+        if (a.net_w) {
+          float x[SN_IN], y[3];
+          const int fi = is_sub ? int(S.code[k] & IK_MASK) : 0;
+          sn_input(a.net_feat + size_t(fi) * SN_FEAT, c, x);
+          __nv_bfloat16* act = reinterpret_cast<__nv_bfloat16*>(&S.u);
+          sn_forward_warp(a.net_w, act, reinterpret_cast<float*>(act + 32 * SN_KS), x, y, lane);
+          s0 = fmin(fmax(double(y[0]), 0.0), 1.0), t0 = fmin(fmax(double(y[1]), 0.0), 1.0);
+        }
         if (k >= n) continue;
         int slot = -1;
         int8_t cert = 0;
@@ -189,7 +200,7 @@ __global__ void __launch_bounds__(WARPS * 32, 2) k_bricks_t(BrickArgs a) {
           cert = sub_convex(s, first, first + mk(8 * h, 8 * h, 8 * h)) ? 1 : 0;
           if (before < MAXSUB) {
             slot = before;
-            S.v.seed[slot] = seed_at(P.sub_cp + 16 * size_t(idx), c);
+            S.v.seed[slot] = seed_at(P.sub_cp + 16 * size_t(idx), c, s0, t0);
           }
         } else if ((S.code[k] >> IK_SHIFT) == IK_FACE) {
           // a plane's trim over the feet of the whole brick (the box's corners projected,

@@ -456,8 +456,10 @@ HD SEf eval_bicubic_f(const float4* cp, float s, float t) {
 // The projected Newton of newton_bicubic in floats (rebased point p), to a step under
 // 1e-6 of the square; the double polish takes it from there.
 // *last: the patch at the point of the last step's start (within that step of the end).
-HDI void newton_bicubic_f(const float4* cp, float3 p, float* ps_, float* pt_, int iters, SEf* last) {
+// Returns whether it converged (a step under 1e-6, or both parameters held).
+HDI bool newton_bicubic_f(const float4* cp, float3 p, float* ps_, float* pt_, int iters, SEf* last) {
   float s = *ps_, t = *pt_;
+  bool conv = false;
   for (int it = 0; it < iters; it++) {
     SEf e = eval_bicubic_f(cp, s, t);
     *last = e;
@@ -468,7 +470,10 @@ HDI void newton_bicubic_f(const float4* cp, float3 p, float* ps_, float* pt_, in
     bool hold_s = (s <= 0.f && g0 > 0.f) || (s >= 1.f && g0 < 0.f);
     bool hold_t = (t <= 0.f && g1 > 0.f) || (t >= 1.f && g1 < 0.f);
     float ds, dt;
-    if (hold_s && hold_t) break;
+    if (hold_s && hold_t) {
+      conv = true;
+      break;
+    }
     if (hold_s) {
       ds = 0.f;
       dt = -g1 / (h2 > 0.f ? h2 : fmaxf(jtt, 1e-30f));
@@ -491,10 +496,23 @@ HDI void newton_bicubic_f(const float4* cp, float3 p, float* ps_, float* pt_, in
     float moved = fabsf(ns - s) + fabsf(nt - t);
     s = ns;
     t = nt;
-    if (moved < 1e-6f) break;
+    if (moved < 1e-6f) {
+      conv = true;
+      break;
+    }
   }
   *ps_ = s;
   *pt_ = t;
+  return conv;
+}
+
+// is_critical at float rounding (1024 units of the last place) for the rebased point p.
+HD bool is_critical_f(float3 p, const SEf& e) {
+  float3 r = f3(e.p.x - p.x, e.p.y - p.y, e.p.z - p.z);
+  float big = fmaxf(fmaxf(fabsf(e.p.x), fabsf(e.p.y)), fabsf(e.p.z)) + fmaxf(fmaxf(fabsf(p.x), fabsf(p.y)), fabsf(p.z));
+  float round = 1024.f * 1.1920929e-7f * (big + sqrtf(dotf(r, r)));
+  float ls = sqrtf(dotf(e.ps, e.ps)), lt = sqrtf(dotf(e.pt, e.pt));
+  return fabsf(dotf(r, e.ps)) <= round * ls && fabsf(dotf(r, e.pt)) <= round * lt;
 }
 
 // surface3.rs:565-572 critical

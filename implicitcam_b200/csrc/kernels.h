@@ -26,6 +26,8 @@ struct BrickArgs {
   const int32_t* leaves;  // the tree's leaf nodes
   int32_t n_leaves;
   int32_t mixed;          // 1: single-precision bulk with double polish
+  const float* net_feat;  // the seed network's sub-patch features and weights
+  const void* net_w;      //   (seednet.cuh), or null: centre starts
   double* d_out;          // optional n x 729 values
   int8_t* flag_out;       // optional n x 729 flags
   uint32_t* words_out;    // optional n x 365 packed words

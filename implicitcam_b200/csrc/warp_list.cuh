@@ -110,8 +110,9 @@ struct Seed {
   double ss[3], st[3];
 };
 
-__device__ __forceinline__ Seed seed_at(const double4* cp, double3 c) {
-  double ss = 0.5, tt = 0.5;
+// Newton starts at (s0, t0): the sub-patch's centre, or a learned start.
+__device__ __forceinline__ Seed seed_at(const double4* cp, double3 c, double s0 = 0.5, double t0 = 0.5) {
+  double ss = s0, tt = t0;
   bool conv;
   newton_bicubic(cp, c, &ss, &tt, 12, &conv);
   SE e = eval_bicubic(cp, ss, tt);
@@ -280,11 +281,25 @@ __device__ __forceinline__ void warp_point(const DPack& P, const WarpCands& W, d
       float3 p32 = f3(float(p.x - s.c[0]), float(p.y - s.c[1]), float(p.z - s.c[2]));
       float sf = float(ss), tf = float(tt);
       SEf ef;
-      newton_bicubic_f(cp32, p32, &sf, &tf, 8, &ef);
+      const bool fconv = newton_bicubic_f(cp32, p32, &sf, &tf, 8, &ef);
       float3 rf = f3(ef.p.x - p32.x, ef.p.y - p32.y, ef.p.z - p32.z);
       double d32 = sqrt(double(dotf(rf, rf)));
       // a float distance past the answer by more than its error cannot win
       if (d32 > best + 1e-4 * (1.0 + best)) continue;
+      // The float answer stands where it is well conditioned: converged, away from the
+      // surface (so its sign is sure; about 2e-6 mm of error on the rebased net, within
+      // the mixed form's 1e-7 of the diagonal) and on a sub-patch wholly inside its
+      // face's loops. Everything else (the sign near zero, the loops' parity near their
+      // edges, a stalled float solve) goes to the double polish below.
+      if (fconv && d32 > 1e-3 && s.klass == 1) {
+        if (!is_critical_f(p32, ef)) continue;
+        float3 nf = f3(ef.ps.y * ef.pt.z - ef.ps.z * ef.pt.y, ef.ps.z * ef.pt.x - ef.ps.x * ef.pt.z,
+                       ef.ps.x * ef.pt.y - ef.ps.y * ef.pt.x);
+        if (!(dotf(nf, nf) > 0.f) || !(d32 < best)) continue;
+        best = d32;
+        sdv = d32 * sgn(-double(dotf(rf, nf)) * P.faces[s.face].sense);
+        continue;
+      }
       ss = sf, tt = tf;
       newton_bicubic(cp64, p, &ss, &tt, 3, &conv);
       if (!conv) newton_bicubic(cp64, p, &ss, &tt, 16, &conv);
