@@ -163,6 +163,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--h", type=float, default=H, help="cell side (mm); smaller cases for profiling")
     ap.add_argument("--band", type=float, default=BAND, help="narrow band half-width (mm), the clamp")
+    ap.add_argument("--seednet-steps", type=int, default=SEEDNET_STEPS,
+                    help="training steps of the seed network (fewer only for profiling captures)")
     args = ap.parse_args()
     set_level(args.h, args.band)
     rank = int(os.environ.get("RANK", 0))
@@ -192,9 +194,9 @@ def main():
     seednet = None
     if prec == part_gpu.MIXED_LEARNED:  # trained before any timing: 50M pairs from the exact evaluator
         t0 = time.perf_counter()
-        loss = g.seednet_train(SEEDNET_STEPS, batch=SEEDNET_BATCH, seed=rank, need=need)
+        loss = g.seednet_train(args.seednet_steps, batch=SEEDNET_BATCH, seed=rank, need=need)
         torch.cuda.synchronize()
-        seednet = {"train_pairs": SEEDNET_STEPS * SEEDNET_BATCH, "train_s": time.perf_counter() - t0,
+        seednet = {"train_pairs": args.seednet_steps * SEEDNET_BATCH, "train_s": time.perf_counter() - t0,
                    "final_loss": float(loss[-50:].mean()), "ab": g.seednet_ab(1 << 20, seed=rank + 7, need=need)}
 
     def step(p, device_only=True, host=None):
