@@ -401,6 +401,57 @@ HDI void newton_bicubic(const double4* cp, double3 p, double* ps_, double* pt_, 
   *pt_ = t;
 }
 
+// newton_bicubic that also hands back the patch at the point it returns, so that the
+// caller needs no evaluation of its own: on a step under 1e-13 it returns the point the
+// step starts from (within that step of the other end; its gradient is within rounding
+// of zero, so the critical-point test reads the same), with both parameters held the
+// point itself. *e is meaningful when *conv.
+HDI void newton_bicubic_e(const double4* cp, double3 p, double* ps_, double* pt_, int iters, bool* conv, SE* e_out) {
+  double s = *ps_, t = *pt_;
+  *conv = false;
+  for (int it = 0; it < iters; it++) {
+    SE e = eval_bicubic(cp, s, t);
+    *e_out = e;
+    double3 r = e.p - p;
+    double g0 = dot(e.ps, r), g1 = dot(e.pt, r);
+    double jss = dot(e.ps, e.ps), jst = dot(e.ps, e.pt), jtt = dot(e.pt, e.pt);
+    double h0 = jss + dot(e.pss, r), h1 = jst + dot(e.pst, r), h2 = jtt + dot(e.ptt, r);
+    bool hold_s = (s <= 0.0 && g0 > 0.0) || (s >= 1.0 && g0 < 0.0);
+    bool hold_t = (t <= 0.0 && g1 > 0.0) || (t >= 1.0 && g1 < 0.0);
+    double ds, dt;
+    if (hold_s && hold_t) {
+      *conv = true;
+      break;
+    }
+    if (hold_s) {
+      ds = 0.0;
+      dt = -g1 / (h2 > 0.0 ? h2 : fmax(jtt, 1e-300));
+    } else if (hold_t) {
+      ds = -g0 / (h0 > 0.0 ? h0 : fmax(jss, 1e-300));
+      dt = 0.0;
+    } else {
+      if (!(h0 > 0.0 && h0 * h2 - h1 * h1 > 0.0)) {
+        h0 = jss;
+        h1 = jst;
+        h2 = jtt;
+      }
+      double det = h0 * h2 - h1 * h1;
+      if (fabs(det) < 1e-300) break;
+      ds = -(h2 * g0 - h1 * g1) / det;
+      dt = -(h0 * g1 - h1 * g0) / det;
+    }
+    double ns = fmin(fmax(s + ds, 0.0), 1.0), nt = fmin(fmax(t + dt, 0.0), 1.0);
+    if (fabs(ns - s) + fabs(nt - t) < 1e-13) {
+      *conv = true;
+      break;
+    }
+    s = ns;
+    t = nt;
+  }
+  *ps_ = s;
+  *pt_ = t;
+}
+
 // ---------------------------------------------------------------- single precision (mixed path)
 
 // The bicubic in floats over control points rebased to the sub-patch's centre: the

@@ -301,16 +301,13 @@ __device__ __forceinline__ void warp_point(const DPack& P, const WarpCands& W, d
         continue;
       }
       ss = sf, tt = tf;
-      newton_bicubic(cp64, p, &ss, &tt, 3, &conv);
-      if (!conv) newton_bicubic(cp64, p, &ss, &tt, 16, &conv);
-    } else {
-      newton_bicubic(cp64, p, &ss, &tt, 16, &conv);
     }
+    SE e;
+    newton_bicubic_e(cp64, p, &ss, &tt, MIXED ? 19 : 16, &conv, &e);
     if (!conv) {
       defer_item(code, lb);
       continue;
     }
-    SE e = eval_bicubic(cp64, ss, tt);
     double d = len(e.p - p);
     if (!(d < best) || !is_critical(p, e)) continue;
     double3 nrm = cross(e.ps, e.pt);
