@@ -74,19 +74,26 @@ HD AxialD axial(const DFace& f, double3 p) {
 // surface3.rs:85-129 foot; surface3.rs:132-148 normal (times the sense); the loops'
 // parameters of the foot (trim2.rs:1904-1933 with the angle itself). Returns false for
 // a singular foot (a cone's apex), where edges and vertices answer.
+HDC bool analytic_foot_curved(const DFace& f, double3 p, double3* q, double3* n, double* u, double* v);
+
+// Planes inline; the curved kinds (with their trigonometry) out of line.
 HDI bool analytic_foot(const DFace& f, double3 p, double3* q, double3* n, double* u, double* v) {
+  if (f.kind == S_PLANE) {
+    double3 z = ld3(f.z);
+    double3 d = p - ld3(f.o);
+    double h = dot(d, z);
+    *q = p - z * h;
+    *n = z * f.sense;
+    double3 e = *q - ld3(f.o);
+    *u = dot(e, ld3(f.x));
+    *v = dot(e, ld3(f.y));
+    return true;
+  }
+  return analytic_foot_curved(f, p, q, n, u, v);
+}
+
+HDC bool analytic_foot_curved(const DFace& f, double3 p, double3* q, double3* n, double* u, double* v) {
   switch (f.kind) {
-    case S_PLANE: {
-      double3 z = ld3(f.z);
-      double3 d = p - ld3(f.o);
-      double h = dot(d, z);
-      *q = p - z * h;
-      *n = z * f.sense;
-      double3 e = *q - ld3(f.o);
-      *u = dot(e, ld3(f.x));
-      *v = dot(e, ld3(f.y));
-      return true;
-    }
     case S_CYLINDER: {
       AxialD ax = axial(f, p);
       *q = ld3(f.o) + ax.er * f.a + ld3(f.z) * ax.h;

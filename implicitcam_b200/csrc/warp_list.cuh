@@ -181,6 +181,35 @@ static __device__ __noinline__ void point_resolve(const DPack& P, double3 p, uin
   *und = B.und;
 }
 
+// A sub-patch's answer at p in double precision: projected Newton from (ss, tt), the
+// critical-point test, a defined normal and (for a sub-patch across its face's loops)
+// the loops' parity; taken into best / sd when nearer. 1 taken, 0 not, 2 the solve did
+// not converge (the caller defers the sub-patch).
+__device__ __forceinline__ int sub_exact(const DPack& P, const double4* cp, const DSub& s, double3 p, double ss,
+                                         double tt, int iters, double* best, double* sd) {
+  SE e;
+  bool conv;
+  newton_bicubic_e(cp, p, &ss, &tt, iters, &conv, &e);
+  if (!conv) return 2;
+  double d = len(e.p - p);
+  if (!(d < *best) || !is_critical(p, e)) return 0;
+  double3 nrm = cross(e.ps, e.pt);
+  if (!(len(nrm) > 0.0)) return 0;
+  if (s.klass != 1 && !trim_inside(P, P.faces[s.face], s.u0 + ss * (s.u1 - s.u0), s.v0 + tt * (s.v1 - s.v0)))
+    return 0;
+  *best = d;
+  *sd = d * sgn(dot(p - e.p, unit(nrm) * P.faces[s.face].sense));
+  return 1;
+}
+static __device__ __noinline__ int sub_exact_cold(const DPack& P, const double4* cp, const DSub& s, double3 p,
+                                                  double ss, double tt, int iters, double* best, double* sd) {
+  return sub_exact(P, cp, s, p, ss, tt, iters, best, sd);
+}
+
+// sub_convex for one point, out of line: most sub-patches are certified for a whole
+// brick at once.
+static __device__ __noinline__ bool sub_convex_at(const DSub& s, double3 p) { return sub_convex(s, p, p); }
+
 // A warp's ranked candidates, in shared memory: code and bound at the centre c, a
 // verdict per candidate (sub-patch: 1 convex over every point the warp asks about;
 // plane: 1 its trim holds at every foot, 2 at none; else 0), the seed slot of each
@@ -267,7 +296,7 @@ __device__ __forceinline__ void warp_point(const DPack& P, const WarpCands& W, d
     const DSub& s = P.subs[idx];
     double lb = box_dist(p, s.box);
     if (lb >= best) continue;
-    if (!W.cert[k] && !sub_convex(s, p, p)) {
+    if (!W.cert[k] && !sub_convex_at(s, p)) {
       defer_item(code, lb);
       continue;
     }
@@ -275,7 +304,6 @@ __device__ __forceinline__ void warp_point(const DPack& P, const WarpCands& W, d
     double ss = 0.5, tt = 0.5;
     if (slot >= 0) seed_params(W.seed[slot], p - c, &ss, &tt);
     const double4* cp64 = W.net;
-    bool conv;
     if (MIXED) {
       const float4* cp32 = W.net32;
       float3 p32 = f3(float(p.x - s.c[0]), float(p.y - s.c[1]), float(p.z - s.c[2]));
@@ -302,20 +330,11 @@ __device__ __forceinline__ void warp_point(const DPack& P, const WarpCands& W, d
       }
       ss = sf, tt = tf;
     }
-    SE e;
-    newton_bicubic_e(cp64, p, &ss, &tt, MIXED ? 19 : 16, &conv, &e);
-    if (!conv) {
-      defer_item(code, lb);
-      continue;
-    }
-    double d = len(e.p - p);
-    if (!(d < best) || !is_critical(p, e)) continue;
-    double3 nrm = cross(e.ps, e.pt);
-    if (!(len(nrm) > 0.0)) continue;
-    if (s.klass != 1 && !trim_inside(P, P.faces[s.face], s.u0 + ss * (s.u1 - s.u0), s.v0 + tt * (s.v1 - s.v0)))
-      continue;
-    best = d;
-    sdv = d * sgn(dot(p - e.p, unit(nrm) * P.faces[s.face].sense));
+    // the double solve: the plain form's every solve, inline; the mixed form's few, out
+    // of line so that its float loop stays small in the instruction cache
+    const int got = MIXED ? sub_exact_cold(P, cp64, s, p, ss, tt, 19, &best, &sdv)
+                          : sub_exact(P, cp64, s, p, ss, tt, 16, &best, &sdv);
+    if (got == 2) defer_item(code, lb);
   }
   if (!live) return;
   if (nd > 0 && nd <= 2 && und < best && und <= cap) point_resolve(P, p, dc0, dl0, dc1, dl1, nd, &best, &sdv, &und);
