@@ -189,6 +189,12 @@ int icam_pack_info(const IcamPack* pk, int64_t counts[7]) {
 
 const char* icam_last_error(const IcamPack* pk) { return pk ? pk->err.c_str() : "null pack"; }
 
+int icam_pack_box(const IcamPack* pk, double lo[3], double hi[3]) {
+  if (!pk || !lo || !hi) return ICAM_ERR_ARG;
+  for (int k = 0; k < 3; k++) lo[k] = pk->host.lo[k], hi[k] = pk->host.hi[k];
+  return ICAM_OK;
+}
+
 void* icam_pack_stream(const IcamPack* pk) { return pk ? static_cast<void*>(pk->stream) : nullptr; }
 
 int icam_points(IcamPack* pk, const double* xyz, size_t n, double clamp, int capped, int precision,
@@ -258,21 +264,21 @@ int icam_bricks(IcamPack* pk, const double* first_nodes, size_t n, double h, dou
   return ICAM_OK;
 }
 
-// The level bake; results left in device scratch.
-static int bake_level(IcamPack* pk, double h, const double lo[3], const int64_t nb[3], double clamp,
-                      const double origin[3], int precision, size_t* n_slots, IcamBakeStats* stats,
-                      const uint32_t** d_map_out, const uint32_t** d_atlas_out) {
-  if (!pk || !lo || !nb || !n_slots) return fail(pk, ICAM_ERR_ARG, "null argument");
+}  // extern "C"
+
+// The level's box decision (partcache.rs:226-331) on the pack's stream, through the
+// read bricks sorted in brick order (partcache.rs:486); results in scratch 3, 9, 10.
+int decide_level(IcamPack* pk, const LevelDesc& L, DecideOut* out) {
+  const double h = L.h, clamp = L.clamp;
+  const double* lo = L.lo;
+  const int64_t* nb = L.nb;
+  const double* origin = L.has_origin ? L.origin : nullptr;
   if (!(h > 0) || !(clamp > 0)) return fail(pk, ICAM_ERR_ARG, "h and clamp must be positive");
   if (nb[0] <= 0 || nb[1] <= 0 || nb[2] <= 0) return fail(pk, ICAM_ERR_ARG, "nb must be positive");
-  if (precision < ICAM_FP64 || precision > ICAM_MIXED_LEARNED) return fail(pk, ICAM_ERR_ARG, "unknown precision");
   CK(cudaSetDevice(pk->device));
   cudaStream_t s = pk->stream;
   int64_t total = nb[0] * nb[1] * nb[2];
   if (total > (int64_t(1) << 34)) return fail(pk, ICAM_ERR_ARG, "level too large");
-  cudaEvent_t ev[5];
-  for (auto& e : ev) CK(cudaEventCreate(&e));
-  CK(cudaEventRecord(ev[0], s));
   int64_t launches = 0;
   void *d_map, *d_cur, *d_next, *d_ridx, *d_rdc, *d_cnt;
   int r;
@@ -341,30 +347,73 @@ static int bake_level(IcamPack* pk, double h, const double lo[3], const int64_t 
   unsigned long long nread = 0;
   CK(cudaMemcpyAsync(&nread, cnt + 1, sizeof(nread), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
-  CK(cudaEventRecord(ev[1], s));
-  int64_t R = int64_t(nread);
+  const int64_t R = int64_t(nread);
   // the read bricks in brick order (partcache.rs:486)
-  void *d_ridx2, *d_rdc2, *d_tmp, *d_first, *d_words, *d_kind, *d_flag, *d_slot, *d_atlas;
+  void *d_ridx2, *d_rdc2, *d_tmp;
   size_t tmp_bytes = 0;
   cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, (int64_t*)nullptr, (int64_t*)nullptr, (double*)nullptr,
                                   (double*)nullptr, R, 0, 64, s);
-  size_t scan_bytes = 0;
-  cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (int64_t*)nullptr, (int64_t*)nullptr, R + 1, s);
-  tmp_bytes = std::max(tmp_bytes, scan_bytes);
-  size_t Rb = size_t(std::max<int64_t>(R, 1));
+  const size_t Rb = size_t(std::max<int64_t>(R, 1));
   if ((r = scratch(pk, 9, Rb * sizeof(int64_t), &d_ridx2)) || (r = scratch(pk, 10, Rb * sizeof(double), &d_rdc2)) ||
-      (r = scratch(pk, 11, tmp_bytes + 16, &d_tmp)) || (r = scratch(pk, 12, Rb * 3 * sizeof(double), &d_first)) ||
+      (r = scratch(pk, 11, tmp_bytes + 16, &d_tmp)))
+    return r;
+  if (R > 0) {
+    CK(cub::DeviceRadixSort::SortPairs(d_tmp, tmp_bytes, (const int64_t*)d_ridx, (int64_t*)d_ridx2,
+                                       (const double*)d_rdc, (double*)d_rdc2, R, 0, 64, s));
+    launches++;
+  }
+  out->map = static_cast<uint32_t*>(d_map);
+  out->read_idx = static_cast<int64_t*>(d_ridx2);
+  out->read_dc = static_cast<double*>(d_rdc2);
+  out->n_read = R;
+  out->boxes_read = boxes_read;
+  out->launches = launches;
+  return ICAM_OK;
+}
+
+extern "C" {
+
+// The level bake; results left in device scratch.
+static int bake_level(IcamPack* pk, double h, const double lo[3], const int64_t nb[3], double clamp,
+                      const double origin[3], int precision, size_t* n_slots, IcamBakeStats* stats,
+                      const uint32_t** d_map_out, const uint32_t** d_atlas_out) {
+  if (!pk || !lo || !nb || !n_slots) return fail(pk, ICAM_ERR_ARG, "null argument");
+  if (precision < ICAM_FP64 || precision > ICAM_MIXED_LEARNED) return fail(pk, ICAM_ERR_ARG, "unknown precision");
+  CK(cudaSetDevice(pk->device));
+  cudaStream_t s = pk->stream;
+  LevelDesc L;
+  L.h = h, L.clamp = clamp;
+  for (int k = 0; k < 3; k++) L.lo[k] = lo[k], L.nb[k] = nb[k], L.origin[k] = origin ? origin[k] : 0.0;
+  L.has_origin = origin != nullptr;
+  cudaEvent_t ev[5];
+  for (auto& e : ev) CK(cudaEventCreate(&e));
+  CK(cudaEventRecord(ev[0], s));
+  DecideOut D;
+  int r = decide_level(pk, L, &D);
+  if (r) {
+    for (auto& e : ev) cudaEventDestroy(e);
+    return r;
+  }
+  CK(cudaEventRecord(ev[1], s));
+  const int64_t R = D.n_read, boxes_read = D.boxes_read;
+  int64_t launches = D.launches;
+  void* d_map = D.map;
+  void *d_tmp, *d_first, *d_words, *d_kind, *d_flag, *d_slot, *d_atlas;
+  size_t tmp_bytes = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, (int64_t*)nullptr, (int64_t*)nullptr, R + 1, s);
+  const size_t Rb = size_t(std::max<int64_t>(R, 1));
+  if ((r = scratch(pk, 11, tmp_bytes + 16, &d_tmp)) || (r = scratch(pk, 12, Rb * 3 * sizeof(double), &d_first)) ||
       (r = scratch(pk, 13, Rb * 365 * sizeof(uint32_t), &d_words)) || (r = scratch(pk, 14, Rb * sizeof(int32_t), &d_kind)) ||
       (r = scratch(pk, 15, (Rb + 1) * 2 * sizeof(int64_t), &d_flag)))
     return r;
   d_slot = (int64_t*)d_flag + (Rb + 1);
+  void* d_ridx2 = D.read_idx;
+  void* d_rdc2 = D.read_dc;
   size_t nwords_slots = 0;
   if (R > 0) {
-    CK(cub::DeviceRadixSort::SortPairs(d_tmp, tmp_bytes, (const int64_t*)d_ridx, (int64_t*)d_ridx2,
-                                       (const double*)d_rdc, (double*)d_rdc2, R, 0, 64, s));
     k_gather_firsts<<<grid_for(R, 256), 256, 0, s>>>((const int64_t*)d_ridx2, R, nb[0], nb[1], h, lo[0], lo[1], lo[2],
                                                     (double*)d_first);
-    launches += 2;
+    launches++;
     CK(cudaEventRecord(ev[2], s));
     BrickArgs b{};
     b.P = pk->dev;

@@ -9,7 +9,7 @@
 
 namespace icam {
 
-constexpr int WARPS = 4;  // bricks a block works on at once, one a warp
+constexpr int MAX_WARPS = 4;  // bricks a block works on at once, one a warp (1, 2 or 4)
 
 // The 26 neighbours of node n inside the brick, in the reference's order (dk, dj, di
 // from -1 to 1, partcache.rs:829-839).
@@ -50,7 +50,7 @@ struct BrickSmem {
   int8_t slot[MAXC];
   int n;
 };
-static_assert(sizeof(BrickSmem) * WARPS <= 48 * 1024, "static shared memory of a block");
+static_assert(sizeof(BrickSmem) * MAX_WARPS <= 48 * 1024, "shared memory of a block");
 static_assert(sizeof(((BrickSmem*)0)->u) >= 32 * SN_KS * 2 + 32 * 8 * 4, "the seed network's room in the list's");
 
 __device__ __forceinline__ uint32_t spread(uint32_t m) { return m | (m << 1) | (m >> 1); }
@@ -125,10 +125,13 @@ __device__ void flood(BrickSmem& S, int lane) {
 //  4. far nodes signed, undecided ones bridged, quantised and packed.
 // Two blocks a SM: the evaluators' register need (255 a thread) left unspilled beats
 // more warps with spills (measured: 8 warps a SM 240 ms, 16 warps 280 ms a bake).
-template <bool MIXED>
-__global__ void __launch_bounds__(WARPS * 32, 2) k_bricks_t(BrickArgs a) {
-  __shared__ BrickSmem smem[WARPS];
-  const DPack& P = a.P;
+// BATCH: bricks of many parts in one launch, each brick's part in a.part_of and that
+// part's pack, level and seed network in a.parts.
+template <bool MIXED, bool BATCH>
+__global__ void __launch_bounds__(MAX_WARPS * 32, 2) k_bricks_t(BrickArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  BrickSmem* smem = reinterpret_cast<BrickSmem*>(smem_raw);
+  const int warps = int(blockDim.x >> 5);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   BrickSmem& S = smem[warp];
   unsigned long long* work = a.stats ? a.stats + 15 : nullptr;
@@ -138,10 +141,16 @@ __global__ void __launch_bounds__(WARPS * 32, 2) k_bricks_t(BrickArgs a) {
       if (lane == 0) b = atomicAdd(work, 1ull);
       return int64_t(__shfl_sync(FULL, b, 0));
     }
-    return cur < 0 ? int64_t(blockIdx.x) * WARPS + warp : cur + int64_t(gridDim.x) * WARPS;
+    return cur < 0 ? int64_t(blockIdx.x) * warps + warp : cur + int64_t(gridDim.x) * warps;
   };
-  const double h = a.h, clamp = a.clamp;
   for (int64_t bi = next_brick(-1); bi < a.n; bi = next_brick(bi)) {
+    const PartParams* Q = BATCH ? a.parts + a.part_of[bi] : nullptr;
+    const DPack& P = BATCH ? Q->P : a.P;
+    const double h = BATCH ? Q->h : a.h, clamp = BATCH ? Q->clamp : a.clamp;
+    const int32_t* leaves = BATCH ? Q->leaves : a.leaves;
+    const int32_t n_leaves = BATCH ? Q->n_leaves : a.n_leaves;
+    const float* net_feat = BATCH ? Q->net_feat : a.net_feat;
+    const void* net_w = BATCH ? Q->net_w : a.net_w;
     double3 first = mk(a.firsts[3 * bi], a.firsts[3 * bi + 1], a.firsts[3 * bi + 2]);
     const double half = 4.0 * h;
     const double3 c = first + mk(half, half, half);
@@ -166,7 +175,7 @@ __global__ void __launch_bounds__(WARPS * 32, 2) k_bricks_t(BrickArgs a) {
       continue;
     }
     // ---- 1. list
-    int n = warp_list(P, a.leaves, a.n_leaves, c, reach, S.u.list.code, S.u.list.lb, S.u.list.fr, &S.n, lane);
+    int n = warp_list(P, leaves, n_leaves, c, reach, S.u.list.code, S.u.list.lb, S.u.list.fr, &S.n, lane);
     const bool overflow = n > MAXC;
     if (overflow) n = MAXC;
     warp_rank(S.u.list.code, S.u.list.lb, n, S.code, S.lb, lane);
@@ -183,12 +192,12 @@ __global__ void __launch_bounds__(WARPS * 32, 2) k_bricks_t(BrickArgs a) {
         // queries (this group of candidates at the centre) on the tensor cores, in the
         // room of the list, which is ranked by now
         double s0 = 0.5, t0 = 0.5;
-        if (a.net_w) {
+        if (net_w) {
           float x[SN_IN], y[3];
           const int fi = is_sub ? int(S.code[k] & IK_MASK) : 0;
-          sn_input(a.net_feat + size_t(fi) * SN_FEAT, c, x);
+          sn_input(net_feat + size_t(fi) * SN_FEAT, c, x);
           __nv_bfloat16* act = reinterpret_cast<__nv_bfloat16*>(&S.u);
-          sn_forward_warp(a.net_w, act, reinterpret_cast<float*>(act + 32 * SN_KS), x, y, lane);
+          sn_forward_warp(net_w, act, reinterpret_cast<float*>(act + 32 * SN_KS), x, y, lane);
           s0 = fmin(fmax(double(y[0]), 0.0), 1.0), t0 = fmin(fmax(double(y[1]), 0.0), 1.0);
         }
         if (k >= n) continue;
@@ -410,15 +419,26 @@ __global__ void __launch_bounds__(WARPS * 32, 2) k_bricks_t(BrickArgs a) {
   }
 }
 
-void launch_bricks(const BrickArgs& a, cudaStream_t s) {
+void launch_bricks(const BrickArgs& a, cudaStream_t s, int warps) {
+  warps = warps == 1 || warps == 2 ? warps : MAX_WARPS;
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int64_t want = (a.n + WARPS - 1) / WARPS;
-  const int grid = int(std::max<int64_t>(1, std::min<int64_t>(want, int64_t(sms) * 2)));
-  if (a.mixed)
-    k_bricks_t<true><<<grid, WARPS * 32, 0, s>>>(a);
-  else
-    k_bricks_t<false><<<grid, WARPS * 32, 0, s>>>(a);
+  // eight warps a SM whatever the block (the register budget), a block per brick at most
+  const int64_t want = (a.n + warps - 1) / warps;
+  const int grid = int(std::max<int64_t>(1, std::min<int64_t>(want, int64_t(sms) * (8 / warps))));
+  const size_t smem = sizeof(BrickSmem) * warps;
+  const bool batch = a.parts != nullptr;
+  if (a.mixed) {
+    if (batch)
+      k_bricks_t<true, true><<<grid, warps * 32, smem, s>>>(a);
+    else
+      k_bricks_t<true, false><<<grid, warps * 32, smem, s>>>(a);
+  } else {
+    if (batch)
+      k_bricks_t<false, true><<<grid, warps * 32, smem, s>>>(a);
+    else
+      k_bricks_t<false, false><<<grid, warps * 32, smem, s>>>(a);
+  }
 }
 
 }  // namespace icam

@@ -17,7 +17,21 @@ struct Box4 {
   double reach;
 };
 
+// One part of a batch (batch.cu): its pack, its level's cell side and clamp, its tree's
+// leaves and its seed network (null: centre starts).
+struct PartParams {
+  DPack P;
+  const int32_t* leaves;
+  int32_t n_leaves;
+  int32_t pad;
+  double h, clamp;
+  const float* net_feat;
+  const void* net_w;
+};
+
 struct BrickArgs {
+  const PartParams* parts;  // a batch: every brick's part in part_of; else null and
+  const int32_t* part_of;   //   the single part's fields below
   DPack P;
   const double* firsts;  // n x 3 first nodes
   const double* dcs;     // n centre distances (NaN when not known), or null
@@ -60,9 +74,13 @@ struct DecideArgs {
 
 __global__ void k_points(DPack P, const double* xyz, int64_t n, double cap, double* value, int8_t* flag);
 
-// The brick kernel (bricks.cu) in the arithmetic a.mixed names, one warp a brick over a
-// grid sized for the current device.
-void launch_bricks(const BrickArgs& a, cudaStream_t s);
+// The brick kernel (bricks.cu) in the arithmetic a.mixed names, one warp a brick, `warps`
+// (1, 2 or 4) a block, over a grid sized for the current device.
+void launch_bricks(const BrickArgs& a, cudaStream_t s, int warps = 4);
+// Map entries and atlas words of a batch's read bricks (batch.cu).
+__global__ void k_assemble_batch(const int64_t* idx, const int32_t* part_of, const int64_t* part_off,
+                                 uint32_t* const* maps, const int32_t* kind, const int64_t* slot, int64_t n,
+                                 const uint32_t* words, uint32_t* atlas);
 // The decision of one box size of a level (decide.cu), 32 boxes a warp.
 void launch_decide(const DecideArgs& a, cudaStream_t s);
 __global__ void k_gather_firsts(const int64_t* idx, int64_t n, int64_t nb0, int64_t nb1, double h, double lo0,

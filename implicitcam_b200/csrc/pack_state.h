@@ -29,6 +29,28 @@ struct SeedNetState {
   bool ready = false;       // weights set (trained or loaded)
 };
 
+// One level of the brick cache to bake: cell side h, first node lo, nb bricks a side,
+// the clamp, and the box grid's origin (the stock's low corner) when there is one.
+struct LevelDesc {
+  double h = 0.0, clamp = 0.0;
+  double lo[3] = {0, 0, 0}, origin[3] = {0, 0, 0};
+  int64_t nb[3] = {0, 0, 0};
+  bool has_origin = false;
+};
+
+// The box decision of a level, left on the device in the pack's scratch: the map (read
+// bricks marked), the read bricks' indices in brick order and their centre distances.
+struct DecideOut {
+  uint32_t* map = nullptr;
+  int64_t* read_idx = nullptr;
+  double* read_dc = nullptr;
+  int64_t n_read = 0, boxes_read = 0, launches = 0;
+};
+
+struct IcamPack;
+// api.cu: the decision (partcache.rs:226-331) through the sort of the read bricks.
+int decide_level(IcamPack* pk, const LevelDesc& L, DecideOut* out);
+
 struct IcamPack {
   int device = 0;
   cudaStream_t stream = nullptr;

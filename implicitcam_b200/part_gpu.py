@@ -42,6 +42,27 @@ class IcamBakeStats(C.Structure):
         return d
 
 
+class IcamBatchLevel(C.Structure):
+    _fields_ = [("h", C.c_double), ("lo", C.c_double * 3), ("nb", C.c_int64 * 3), ("clamp", C.c_double),
+                ("origin", C.c_double * 3), ("has_origin", C.c_int32), ("pad", C.c_int32)]
+
+
+class IcamBatchPart(C.Structure):
+    _fields_ = [("d_map", C.c_void_p), ("d_atlas", C.c_void_p), ("n_slots", C.c_size_t), ("bricks_read", C.c_int64)]
+
+
+class IcamBatchStats(C.Structure):
+    _fields_ = [("parts", C.c_int64), ("boxes_read", C.c_int64), ("bricks_read", C.c_int64),
+                ("bricks_words", C.c_int64), ("nodes_exact", C.c_int64), ("nodes_undecided", C.c_int64),
+                ("kernel_launches", C.c_int64), ("warps", C.c_int32), ("graph_replayed", C.c_int32),
+                ("tune_ms", C.c_double * 3), ("ms_decide", C.c_double), ("ms_bricks", C.c_double)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "tune_ms"}
+        d["tune_ms"] = list(self.tune_ms)
+        return d
+
+
 def lib():
     """The CUDA library, loaded once (raises when it is missing: build it with
     ``python -m implicitcam_b200.build``)."""
@@ -73,6 +94,13 @@ def lib():
         L.icam_seednet_grad.argtypes = [vp, vp, vp, sz, vp, C.POINTER(d)]
         L.icam_seednet_train.argtypes = [vp, C.c_int64, C.c_int64, u64, d, d, vp]
         L.icam_seednet_ab.argtypes = [vp, sz, u64, d, vp]
+        L.icam_pack_box.argtypes = [vp, vp, vp]
+        L.icam_batch_create.argtypes = [vp, sz, C.POINTER(vp), C.c_char_p, sz]
+        L.icam_batch_destroy.argtypes = [vp]
+        L.icam_batch_bake.argtypes = [vp, vp, C.c_int, vp, vp]
+        L.icam_batch_read.argtypes = [vp, vp, sz, vp, vp, sz]
+        L.icam_batch_last_error.restype = C.c_char_p
+        L.icam_batch_last_error.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -112,6 +140,12 @@ class PartGpu:
     def _check(self, rc, what):
         if rc != 0:
             raise IcamError(f"{what}: {rc}: {lib().icam_last_error(self.h).decode()}")
+
+    def box(self):
+        """The solid's box (lo, hi)."""
+        lo, hi = np.zeros(3), np.zeros(3)
+        self._check(lib().icam_pack_box(self.h, _p(lo), _p(hi)), "icam_pack_box")
+        return lo, hi
 
     def info(self):
         c = np.zeros(7, np.int64)
@@ -267,3 +301,56 @@ def unpack_atlas(atlas):
     q[:, 0::2] = lo
     q[:, 1::2] = hi
     return q[:, :729]
+
+
+class Batch:
+    """Many parts baked together (icam_batch_*, include/icam_cuda.h): each part's box
+    decision on its own pack, then all parts' bricks in one launch of the brick kernel,
+    the rest replayed as a CUDA graph. No counterpart in the reference."""
+
+    def __init__(self, parts):
+        self.parts = list(parts)
+        arr = (C.c_void_p * len(self.parts))(*[p.h for p in self.parts])
+        h = C.c_void_p()
+        err = C.create_string_buffer(512)
+        rc = lib().icam_batch_create(arr, len(self.parts), C.byref(h), err, 512)
+        if rc != 0:
+            raise IcamError(f"icam_batch_create: {rc}: {err.value.decode()}")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().icam_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def bake(self, levels, precision=FP64, read=True):
+        """levels: per part (h, lo, nb, clamp[, origin]). Returns the stats and, with
+        read, every part's (map, atlas) in host memory."""
+        n = len(self.parts)
+        lv = (IcamBatchLevel * n)()
+        for i, L in enumerate(levels):
+            h, lo, nb, clamp = L[:4]
+            origin = L[4] if len(L) > 4 else None
+            lv[i].h, lv[i].clamp = float(h), float(clamp)
+            for k in range(3):
+                lv[i].lo[k], lv[i].nb[k] = float(lo[k]), int(nb[k])
+                lv[i].origin[k] = float(origin[k]) if origin is not None else 0.0
+            lv[i].has_origin = int(origin is not None)
+        out = (IcamBatchPart * n)()
+        st = IcamBatchStats()
+        rc = lib().icam_batch_bake(self.h, lv, precision, out, C.byref(st))
+        if rc != 0:
+            raise IcamError(f"icam_batch_bake: {rc}: {lib().icam_batch_last_error(self.h).decode()}")
+        res = []
+        if read:
+            for i, L in enumerate(levels):
+                m = np.zeros(int(np.prod(L[2])), np.uint32)
+                a = np.zeros(max(out[i].n_slots, 1) * WORDS, np.uint32)
+                rc = lib().icam_batch_read(self.h, C.byref(out[i]), len(m), _p(m), _p(a), len(a))
+                if rc != 0:
+                    raise IcamError(f"icam_batch_read: {rc}: {lib().icam_batch_last_error(self.h).decode()}")
+                res.append((m, a[: out[i].n_slots * WORDS].reshape(-1, WORDS)))
+        return st.as_dict(), res

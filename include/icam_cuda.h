@@ -164,6 +164,58 @@ void* icam_pack_stream(const IcamPack* pack);
 /* The last error message of a call on this pack. */
 const char* icam_last_error(const IcamPack* pack);
 
+/* The solid's box (Exact's tree root, solid3.rs:97-236). */
+int icam_pack_box(const IcamPack* pack, double lo[3], double hi[3]);
+
+/* ---- Batches: many parts baked together. No counterpart in the reference, which bakes
+ * one part a call (PartCache::level, partcache.rs:433). Each part's box decision runs on
+ * its own pack; then every part's read bricks go through one launch of the brick kernel
+ * fed by a device work queue, one scan and one assembly, captured as a CUDA graph and
+ * replayed while the batch's levels and sizes stay the same. The brick kernel's tiling
+ * (warps a block) is picked by timing each choice on the batch's first bake. A part's
+ * results are the same as icam_bake_level_device's for that part alone. */
+typedef struct IcamBatch IcamBatch;
+
+typedef struct IcamBatchLevel { /* one part's level, as icam_bake_level takes it */
+  double h;
+  double lo[3];
+  int64_t nb[3];
+  double clamp;
+  double origin[3];
+  int32_t has_origin;
+  int32_t pad;
+} IcamBatchLevel;
+
+typedef struct IcamBatchPart { /* one part's level, in device memory */
+  const uint32_t* d_map;       /* nb[0] x nb[1] x nb[2] entries (in the part's pack) */
+  const uint32_t* d_atlas;     /* n_slots x 365 words (in the batch) */
+  size_t n_slots;
+  int64_t bricks_read;
+} IcamBatchPart;
+
+typedef struct IcamBatchStats {
+  int64_t parts, boxes_read, bricks_read, bricks_words, nodes_exact, nodes_undecided;
+  int64_t kernel_launches;
+  int32_t warps;           /* the tiling in use: warps a block of the brick kernel */
+  int32_t graph_replayed;  /* 1: the post-decision graph was replayed, 0: captured */
+  double tune_ms[3];       /* the tuning's times for 1, 2 and 4 warps a block */
+  double ms_decide, ms_bricks;
+} IcamBatchStats;
+
+/* A batch over n packs (distinct, one device). The packs must outlive it, and no other
+ * call may use them while a batch bake runs (their scratch holds its decisions). */
+int icam_batch_create(IcamPack* const* packs, size_t n, IcamBatch** out, char* err, size_t errlen);
+void icam_batch_destroy(IcamBatch* batch);
+/* Bakes levels[i] of part i, all parts together; parts_out[i] its results, valid until
+ * the next bake of the batch or of the part's pack. */
+int icam_batch_bake(IcamBatch* batch, const IcamBatchLevel* levels, int precision, IcamBatchPart* parts_out,
+                    IcamBatchStats* stats);
+const char* icam_batch_last_error(const IcamBatch* batch);
+/* A part's map (map_entries of them) and atlas (atlas_cap_words >= its n_slots x 365)
+ * copied to host arrays. */
+int icam_batch_read(IcamBatch* batch, const IcamBatchPart* part, size_t map_entries, uint32_t* map_out,
+                    uint32_t* atlas_out, size_t atlas_cap_words);
+
 /* ---- The seed network (ICAM_MIXED_LEARNED). No counterpart in the reference, which
  * starts every Newton solve on a B-spline sub-patch at its centre: a small MLP
  * (query in the sub-patch's frame + a 16-number descriptor -> 64 -> 64 -> 64 ->
