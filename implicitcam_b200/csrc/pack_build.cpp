@@ -124,7 +124,9 @@ bool build_pack(const IcamSolidDesc* d, double need, HostPack* hp, std::string* 
   HostPack& P = *hp;
   P = HostPack();
   P.tol = d->tol;
-  if (d->n_faces <= 0 || d->n_edges <= 0 || d->n_verts <= 0) {
+  // A closed face (a sphere, a torus) has no edges and no vertices: only faces are required.
+  if (d->n_faces <= 0 || d->n_edges < 0 || d->n_verts < 0 || (d->n_edges > 0 && !d->edges) ||
+      (d->n_verts > 0 && !d->verts)) {
     *err = "empty solid";
     return false;
   }

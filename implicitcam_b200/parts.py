@@ -8,7 +8,9 @@
   at its centre (6 planes + 1 cylinder);
 - ``freeform_top``: a 120 x 120 x 50 mm block whose top face is a clamped bicubic
   rational B-spline with 16 x 16 control points, heights 50 mm plus 8 seeded
-  Gaussian bumps, weights in [0.8, 1.2].
+  Gaussian bumps, weights in [0.8, 1.2];
+- ``frustum``, ``ball``, ``ring``: a cone-sided can, a sphere and a torus, the analytic
+  surface kinds the parts above lack (the sphere and torus have no edges at all).
 
 Random numbers come from the reference checkers' xorshift64 generator
 (crates/icam-check/src/exact_check.rs:45-52) seeded through splitmix64, so that
@@ -21,8 +23,8 @@ import math
 import numpy as np
 
 from .solid import (
-    CYLINDER, NURBS, PLANE, Frame, SolidBuilder, arc_pcurve, elevate_to_cubic, line_pcurve,
-    surface_spans,
+    CONE, CYLINDER, NURBS, PLANE, SPHERE, TORUS, Frame, SolidBuilder, arc_pcurve, elevate_to_cubic,
+    line_pcurve, surface_spans,
 )
 
 TAU = 2.0 * math.pi
@@ -289,6 +291,49 @@ def freeform_top(seed=0, n=16, size=120.0, base=50.0, bumps=8):
     knots = [0.0] * 4 + [k / spans for k in range(1, spans)] + [1.0] * 4
     b = SolidBuilder(tol=1e-9)
     return _nurbs_box(b, 3, 3, knots, knots, net, size, size)
+
+
+def frustum(r0=2.0, half_angle_deg=20.0, height=4.0):
+    """The can with a cone for its side: radius r0 at z = 0 widening to
+    r0 + height tan(angle) at z = height (two planes, one cone, two circles, one seam)."""
+    b = SolidBuilder(tol=1e-9)
+    ang = math.radians(half_angle_deg)
+    r1 = r0 + height * math.tan(ang)
+    z, x = [0, 0, 1], [1, 0, 0]
+    f0 = Frame([0, 0, 0], z, x)
+    f1 = Frame([0, 0, height], z, x)
+    va = b.vertex([r0, 0, 0])
+    vb = b.vertex([r1, 0, height])
+    c0 = b.arc(f0, r0, 0.0, TAU, va, va)
+    c1 = b.arc(f1, r1, 0.0, TAU, vb, vb)
+    seam = b.line(va, vb)
+    _plane_face(b, f0, -1, [[(c0, True)]])
+    _plane_face(b, f1, +1, [[(c1, False)]])
+    lo, hi = _pad([0.0, 0.0], [TAU, height])
+    cone = b.face(CONE, +1, f0, a=r0, b=ang, lo=[0.0, lo[1]], hi=[TAU, hi[1]], period=[TAU, 0.0])
+    b.loop(cone, [
+        (c0, False, line_pcurve([0.0, 0.0], [TAU, 0.0])),
+        (seam, False, None),
+        (c1, True, line_pcurve([TAU, height], [0.0, height])),
+        (seam, True, None),
+    ])
+    return b
+
+
+def ball(r=3.0, center=(0.0, 0.0, 0.0)):
+    """A sphere: one face, no loops, no edges, no vertices."""
+    b = SolidBuilder(tol=1e-9)
+    b.face(SPHERE, +1, Frame(list(center), [0, 0, 1], [1, 0, 0]), a=r, lo=[0.0, -math.pi / 2],
+           hi=[TAU, math.pi / 2], period=[TAU, 0.0])
+    return b
+
+
+def ring(major=4.0, minor=1.5):
+    """A torus about z: one face, periodic both ways, no loops, no edges, no vertices."""
+    b = SolidBuilder(tol=1e-9)
+    b.face(TORUS, +1, Frame([0, 0, 0], [0, 0, 1], [1, 0, 0]), a=major, b=minor, lo=[0.0, -math.pi],
+           hi=[TAU, math.pi], period=[TAU, TAU])
+    return b
 
 
 CONFIGS = {
