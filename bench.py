@@ -320,21 +320,30 @@ def main():
 
 
 def batch_parts(seed0=0, count=64):
-    """Uneven seeded parts: rational B-spline tops of 4 x 4 to 32 x 32 control points
-    and 20-120 mm sides, blocks with holes, cans (planes, cylinders, B-splines)."""
+    """Uneven seeded parts of four families, a quarter each: blocks with rational
+    B-spline tops of 4 x 4 to 32 x 32 control points and 20-120 mm sides; bosses
+    (cylinder, torus fillet, plane cap); blocks with countersunk holes (cylinder and
+    cone); spherical domes (cylinder under a hemisphere). Returns [(family, solid)]."""
     from implicitcam_b200 import parts
 
     out = []
     for k in range(count):
         f = k % 4
-        if f in (0, 1):
-            out.append(parts.freeform_top(seed=seed0 + k, n=4 + (7 * k) % 29, size=20.0 + (37 * k) % 100,
-                                          base=10.0 + (13 * k) % 40, bumps=2 + k % 7))
+        if f == 0:
+            out.append(("freeform_top", parts.freeform_top(
+                seed=seed0 + k, n=4 + (7 * k) % 29, size=20.0 + (37 * k) % 100, base=10.0 + (13 * k) % 40,
+                bumps=2 + k % 7)))
+        elif f == 1:
+            r = 4.0 + (5 * k) % 17
+            out.append(("boss", parts.boss(r=r, height=r + 4.0 + (3 * k) % 19, fillet=0.5 + 0.1 * ((7 * k) % 20))))
         elif f == 2:
             X, Y, Z = 20.0 + (11 * k) % 80, 15.0 + (7 * k) % 50, 10.0 + (5 * k) % 30
-            out.append(parts.block_with_hole(size=(X, Y, Z), center=(X / 2, Y / 2), r=0.15 * min(X, Y)))
+            r = 0.12 * min(X, Y)
+            out.append(("countersunk_block", parts.countersunk_block(
+                size=(X, Y, Z), center=(X / 2, Y / 2), r=r, sink=min(0.4 * r, 0.3 * Z))))
         else:
-            out.append(parts.can(r=2.0 + k % 5, height=3.0 + k % 7))
+            r = 3.0 + (7 * k) % 23
+            out.append(("dome", parts.dome(r=r, height=2.0 + (5 * k) % 21)))
     return out
 
 
@@ -349,8 +358,8 @@ def run_batch(args, rank, world):
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
     h, band = 0.2, 1.0
     prec = {"fp64": part_gpu.FP64, "mixed": part_gpu.MIXED, "learned": part_gpu.MIXED}[args.precision]
-    gs, levels, faces = [], [], []
-    for solid in batch_parts(seed0=64 * rank):
+    gs, levels, faces, fams = [], [], [], []
+    for fam, solid in batch_parts(seed0=64 * rank):
         # certificates for points within the band (a node reads a sub-patch only nearer
         # than the clamp); the brick-wide margin would split these curved tops far deeper
         g = part_gpu.PartGpu(solid, need=band)
@@ -360,6 +369,7 @@ def run_batch(args, rank, world):
         gs.append(g)
         levels.append((h, lo2, nb, band))
         faces.append(g.info()["faces"])
+        fams.append(fam)
     batch = part_gpu.Batch(gs)
     for _ in range(args.warmup):
         batch.bake(levels, precision=prec, read=False)
@@ -391,6 +401,10 @@ def run_batch(args, rank, world):
                           "bricks_read_min_max": [min(per_part), max(per_part)], "precision": args.precision},
                "one_part_at_a_time": {"value": voxels / t_alone, "ms_per_step": 1e3 * t_alone},
                "speedup_vs_one_at_a_time": t_alone / t_batch,
+               "families": {fam: {"parts": fams.count(fam),
+                                  "faces": sum(n for n, f in zip(faces, fams) if f == fam),
+                                  "bricks_read": sum(n for n, f in zip(per_part, fams) if f == fam)}
+                            for fam in sorted(set(fams))},
                "batch_stats": {k: st[k] for k in ("bricks_read", "bricks_words", "warps", "graph_replayed",
                                                   "tune_ms", "ms_decide", "ms_bricks", "kernel_launches")}}
         print(json.dumps(out), flush=True)

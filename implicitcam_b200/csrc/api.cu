@@ -268,11 +268,38 @@ int icam_bricks(IcamPack* pk, const double* first_nodes, size_t n, double h, dou
 
 // The level's box decision (partcache.rs:226-331) on the pack's stream, through the
 // read bricks sorted in brick order (partcache.rs:486); results in scratch 3, 9, 10.
+// The first boxes of a level's decision, on the grid aligned on the origin
+// (partcache.rs:250-270); returns their size in bricks.
+long long first_boxes(const LevelDesc& L, std::vector<Box4>* out) {
+  const int64_t* nb = L.nb;
+  const double* lo = L.lo;
+  const double* origin = L.has_origin ? L.origin : nullptr;
+  long long nbmax = std::max(nb[0], std::max(nb[1], nb[2]));
+  long long size = 1;
+  // The reference starts from one box over the whole level; here from boxes of at most
+  // 32 bricks a side (measured on the freeform part at h = 0.1: decide 56 -> 44 ms). Every box a coarser start would settle is settled the same way by
+  // the boxes inside it (grown by the clamp, a child's ball lies in its parent's), so the
+  // map is the same, and the few coarse boxes, each read within tens of mm, are spared.
+  while (size < nbmax && size < 32) size *= 2;
+  double side = 8.0 * L.h;
+  double o[3] = {origin ? origin[0] - L.h : lo[0] - 0.0, origin ? origin[1] - L.h : lo[1], origin ? origin[2] - L.h : lo[2]};
+  long long g0[3], start[3];
+  for (int k = 0; k < 3; k++) {
+    g0[k] = origin ? (long long)std::llround((lo[k] - o[k]) / side) : 0;
+    long long q = g0[k] >= 0 ? g0[k] / size : -((-g0[k] + size - 1) / size);
+    start[k] = q * size - g0[k];
+  }
+  out->clear();
+  for (long long z = start[2]; z < nb[2]; z += size)
+    for (long long y = start[1]; y < nb[1]; y += size)
+      for (long long x = start[0]; x < nb[0]; x += size) out->push_back({x, y, z, NAN, INFINITY});
+  return size;
+}
+
 int decide_level(IcamPack* pk, const LevelDesc& L, DecideOut* out) {
   const double h = L.h, clamp = L.clamp;
   const double* lo = L.lo;
   const int64_t* nb = L.nb;
-  const double* origin = L.has_origin ? L.origin : nullptr;
   if (!(h > 0) || !(clamp > 0)) return fail(pk, ICAM_ERR_ARG, "h and clamp must be positive");
   if (nb[0] <= 0 || nb[1] <= 0 || nb[2] <= 0) return fail(pk, ICAM_ERR_ARG, "nb must be positive");
   CK(cudaSetDevice(pk->device));
@@ -289,26 +316,8 @@ int decide_level(IcamPack* pk, const LevelDesc& L, DecideOut* out) {
       (r = scratch(pk, 7, total * sizeof(double), &d_rdc)) || (r = scratch(pk, 8, 4 * sizeof(unsigned long long), &d_cnt)))
     return r;
   CK(cudaMemsetAsync(d_cnt, 0, 4 * sizeof(unsigned long long), s));
-  // the first boxes, on the grid aligned on the origin (partcache.rs:250-270)
-  long long nbmax = std::max(nb[0], std::max(nb[1], nb[2]));
-  long long size = 1;
-  // The reference starts from one box over the whole level; here from boxes of at most
-  // 32 bricks a side (measured on the freeform part at h = 0.1: decide 56 -> 44 ms). Every box a coarser start would settle is settled the same way by
-  // the boxes inside it (grown by the clamp, a child's ball lies in its parent's), so the
-  // map is the same, and the few coarse boxes, each read within tens of mm, are spared.
-  while (size < nbmax && size < 32) size *= 2;
-  double side = 8.0 * h;
-  double o[3] = {origin ? origin[0] - h : lo[0] - 0.0, origin ? origin[1] - h : lo[1], origin ? origin[2] - h : lo[2]};
-  long long g0[3], start[3];
-  for (int k = 0; k < 3; k++) {
-    g0[k] = origin ? (long long)std::llround((lo[k] - o[k]) / side) : 0;
-    long long q = g0[k] >= 0 ? g0[k] / size : -((-g0[k] + size - 1) / size);
-    start[k] = q * size - g0[k];
-  }
   std::vector<Box4> first;
-  for (long long z = start[2]; z < nb[2]; z += size)
-    for (long long y = start[1]; y < nb[1]; y += size)
-      for (long long x = start[0]; x < nb[0]; x += size) first.push_back({x, y, z, NAN, INFINITY});
+  long long size = first_boxes(L, &first);
   CK(cudaMemcpyAsync(d_cur, first.data(), first.size() * sizeof(Box4), cudaMemcpyHostToDevice, s));
   int64_t ncur = int64_t(first.size()), boxes_read = 0;
   unsigned long long* cnt = (unsigned long long*)d_cnt;

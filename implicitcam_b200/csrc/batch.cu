@@ -1,7 +1,9 @@
-// Many parts baked together: each part's box decision on its own pack (host-driven, box
-// size by box size), then every part's read bricks through ONE launch of the brick
-// kernel fed by a device work queue (an atomic brick counter over all parts), one scan
-// numbering the stored bricks and one assembly into every part's map and a shared atlas.
+// Many parts baked together: every part's box decision in one launch a box size (warps
+// take groups of 32 boxes of one part across all parts; no host synchronisation between
+// sizes), one sort of all parts' read bricks, then every part's read bricks through ONE
+// launch of the brick kernel fed by a device work queue (an atomic brick counter over all
+// parts), one scan numbering the stored bricks and one assembly into every part's map and
+// a shared atlas.
 // The part after the decisions is captured as a CUDA graph and replayed while the batch's
 // levels and sizes stay the same; the brick kernel's tiling (warps a block) is picked by
 // timing each choice on the batch's first bake. No counterpart in the reference, which
@@ -24,9 +26,42 @@ using namespace icam;
 
 namespace icam {
 
-__global__ void k_fill_part(int32_t* part_of, int64_t n, int32_t part) {
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
-    part_of[i] = part;
+constexpr int PART_SHIFT = 34;  // a read brick's sort key: part << PART_SHIFT | brick index
+
+// Every part's read bricks (part p's n_read[p] at read_off[p]) as dense sort keys and
+// centre distances: dense position j of part p is off[p] + its rank in the part's list.
+__global__ void k_batch_keys(const int64_t* read_idx, const double* read_dc, const int64_t* read_off,
+                             const int64_t* off, int n_parts, int64_t R, uint64_t* keys, double* dcs) {
+  for (int64_t j = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; j < R; j += int64_t(gridDim.x) * blockDim.x) {
+    int lo = 0, hi = n_parts;  // off[lo] <= j < off[lo + 1]
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) / 2;
+      if (off[mid] <= j) lo = mid;
+      else hi = mid;
+    }
+    const int64_t src = read_off[lo] + (j - off[lo]);
+    keys[j] = (uint64_t(lo) << PART_SHIFT) | uint64_t(read_idx[src]);
+    dcs[j] = read_dc[src];
+  }
+}
+
+// The sorted keys split into brick indices, parts and first nodes (as k_gather_firsts).
+__global__ void k_batch_split(const uint64_t* keys, int64_t R, const DecideArgs* args, int64_t* idx, int32_t* part_of,
+                              double* firsts) {
+  for (int64_t j = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; j < R; j += int64_t(gridDim.x) * blockDim.x) {
+    const uint64_t k = keys[j];
+    const int p = int(k >> PART_SHIFT);
+    const int64_t b = int64_t(k & ((uint64_t(1) << PART_SHIFT) - 1));
+    const DecideArgs& a = args[2 * p];
+    const int64_t nb0 = a.nb[0], nb1 = a.nb[1];
+    const int64_t x = b % nb0, y = (b / nb0) % nb1, z = b / (nb0 * nb1);
+    const double side = 8.0 * a.h;
+    idx[j] = b;
+    part_of[j] = p;
+    firsts[3 * j] = a.lo[0] + side * x;
+    firsts[3 * j + 1] = a.lo[1] + side * y;
+    firsts[3 * j + 2] = a.lo[2] + side * z;
+  }
 }
 
 // The stored-brick number of each part's first brick (slot at its offset), n + 1 values.
@@ -60,7 +95,7 @@ struct IcamBatch {
     void* p = nullptr;
     size_t n = 0;
   };
-  Buf buf[12];
+  Buf buf[24];
   PartParams* d_parts = nullptr;
   unsigned long long* d_stats = nullptr;
   int warps = 0;  // the tuned tiling (0: not tuned yet)
@@ -119,11 +154,6 @@ int icam_batch_create(IcamPack* const* packs, size_t n, IcamBatch** out, char* e
       report("every pack of a batch must exist and be on one device");
       return ICAM_ERR_ARG;
     }
-    for (size_t j = 0; j < i; j++)
-      if (packs[j] == packs[i]) {  // its decision lives in the pack's scratch until the bricks run
-        report("a pack may be in a batch once");
-        return ICAM_ERR_ARG;
-      }
   }
   IcamBatch* bt = new IcamBatch();
   bt->device = packs[0]->device;
@@ -190,67 +220,163 @@ int icam_batch_bake(IcamBatch* bt, const IcamBatchLevel* levels, int precision, 
     for (auto& e : ev) cudaEventDestroy(e);
   };
   BCK(cudaEventRecord(ev[0], s));
-  // every part's decision, on its own pack and stream
-  std::vector<DecideOut> D(n);
-  std::vector<int64_t> off(n + 1, 0);
-  int64_t launches = 0, boxes = 0;
+  // every part's decision together: first boxes, regions of the box lists, maps and read
+  // lists at per-part offsets, then one launch pair a box size
+  std::vector<DecideArgs> args(2 * n);
+  std::vector<std::vector<Box4>> first(n);
+  std::vector<int64_t> box_off(n + 1, 0), lvl_off(n + 1, 0);
+  int rounds = 0;
   for (int i = 0; i < n; i++) {
     IcamPack* pk = bt->packs[i];
     const IcamBatchLevel& lv = levels[i];
-    LevelDesc L;
-    L.h = lv.h, L.clamp = lv.clamp;
-    for (int k = 0; k < 3; k++) L.lo[k] = lv.lo[k], L.nb[k] = lv.nb[k], L.origin[k] = lv.origin[k];
-    L.has_origin = lv.has_origin != 0;
+    if (!(lv.h > 0) || !(lv.clamp > 0) || lv.nb[0] <= 0 || lv.nb[1] <= 0 || lv.nb[2] <= 0) {
+      cleanup();
+      return bfail(bt, ICAM_ERR_ARG, "part " + std::to_string(i) + ": h, clamp and nb must be positive");
+    }
+    const int64_t total = lv.nb[0] * lv.nb[1] * lv.nb[2];
+    if (total > (int64_t(1) << PART_SHIFT)) {
+      cleanup();
+      return bfail(bt, ICAM_ERR_ARG, "part " + std::to_string(i) + ": level too large");
+    }
     if (precision == ICAM_MIXED_LEARNED && !pk->net.ready) {
       cleanup();
       return bfail(bt, ICAM_ERR_ARG, "ICAM_MIXED_LEARNED: part " + std::to_string(i) + " has no trained seed network");
     }
-    int r = decide_level(pk, L, &D[i]);
-    if (r == ICAM_OK && cudaStreamSynchronize(pk->stream) != cudaSuccess) r = ICAM_ERR_CUDA;  // its sort done
-    if (r) {
-      cleanup();
-      return bfail(bt, r, "part " + std::to_string(i) + ": " + pk->err);
-    }
-    off[i + 1] = off[i] + D[i].n_read;
-    launches += D[i].launches;
-    boxes += D[i].boxes_read;
+    BCK(cudaStreamSynchronize(pk->stream));  // the pack's uploads and training done
+    LevelDesc L;
+    L.h = lv.h, L.clamp = lv.clamp;
+    for (int k = 0; k < 3; k++) L.lo[k] = lv.lo[k], L.nb[k] = lv.nb[k], L.origin[k] = lv.origin[k];
+    L.has_origin = lv.has_origin != 0;
+    const long long size = first_boxes(L, &first[i]);
+    int lg = 0;
+    while ((1LL << lg) < size) lg++;
+    rounds = std::max(rounds, lg + 1);
+    // box lists: boxes of one size are disjoint and each holds a brick of the level
+    box_off[i + 1] = box_off[i] + std::max<int64_t>(total + 64, 1 << 12);
+    lvl_off[i + 1] = lvl_off[i] + total;
+    DecideArgs& a = args[2 * i];
+    a.P = pk->dev;
+    a.leaves = pk->leaves;
+    a.n_leaves = int32_t(pk->leaves_host.size());
+    a.size = size;
+    a.h = lv.h;
+    a.clamp = lv.clamp;
+    for (int k = 0; k < 3; k++) a.lo[k] = lv.lo[k], a.nb[k] = lv.nb[k];
+    a.next_cap = box_off[i + 1] - box_off[i];
+    a.read_cap = total;
   }
-  BCK(cudaEventRecord(ev[1], s));
+  void *boxes[2], *maps_all, *ridx, *rdc, *cnt, *groups, *d_args, *d_roff, *keys[2];
+  const int64_t BX = box_off[n], LV = lvl_off[n];
+  int r;
+  if ((r = bbuf(bt, 12, BX * sizeof(Box4), &boxes[0])) || (r = bbuf(bt, 13, BX * sizeof(Box4), &boxes[1])) ||
+      (r = bbuf(bt, 14, LV * sizeof(uint32_t), &maps_all)) || (r = bbuf(bt, 15, LV * sizeof(int64_t), &ridx)) ||
+      (r = bbuf(bt, 16, LV * sizeof(double), &rdc)) ||
+      (r = bbuf(bt, 17, (3 * n + 2) * sizeof(unsigned long long), &cnt)) ||
+      (r = bbuf(bt, 18, (n + 1) * sizeof(int64_t), &groups)) || (r = bbuf(bt, 19, 2 * n * sizeof(DecideArgs), &d_args)) ||
+      (r = bbuf(bt, 20, (n + 1) * sizeof(int64_t), &d_roff))) {
+    cleanup();
+    return r;
+  }
+  unsigned long long* c = static_cast<unsigned long long*>(cnt);  // 2n box counts, n read counts, boxes, error
+  std::vector<unsigned long long> c0(3 * n + 2, 0);
+  std::vector<uint32_t*> maps(n);
+  for (int i = 0; i < n; i++) {
+    DecideArgs& a = args[2 * i];
+    maps[i] = static_cast<uint32_t*>(maps_all) + lvl_off[i];
+    a.map = maps[i];
+    a.read_idx = static_cast<int64_t*>(ridx) + lvl_off[i];
+    a.read_dc = static_cast<double*>(rdc) + lvl_off[i];
+    a.n_read = c + 2 * n + i;
+    DecideArgs& b = args[2 * i + 1];
+    b = a;
+    a.boxes = static_cast<Box4*>(boxes[0]) + box_off[i];
+    a.next = static_cast<Box4*>(boxes[1]) + box_off[i];
+    a.n_next = c + 2 * i + 1;
+    b.boxes = static_cast<Box4*>(boxes[1]) + box_off[i];
+    b.next = static_cast<Box4*>(boxes[0]) + box_off[i];
+    b.n_next = c + 2 * i;
+    c0[2 * i] = first[i].size();
+    if (!first[i].empty())
+      BCK(cudaMemcpyAsync(static_cast<Box4*>(boxes[0]) + box_off[i], first[i].data(), first[i].size() * sizeof(Box4),
+                          cudaMemcpyHostToDevice, s));
+  }
+  BCK(cudaMemcpyAsync(c, c0.data(), c0.size() * sizeof(unsigned long long), cudaMemcpyHostToDevice, s));
+  BCK(cudaMemcpyAsync(d_args, args.data(), args.size() * sizeof(DecideArgs), cudaMemcpyHostToDevice, s));
+  BCK(cudaMemcpyAsync(d_roff, lvl_off.data(), (n + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+  DecideBatchArgs db{};
+  db.args = static_cast<const DecideArgs*>(d_args);
+  db.n_parts = n;
+  db.cnt = c;
+  db.groups = static_cast<int64_t*>(groups);
+  db.boxes_read = c + 3 * n;
+  db.err = reinterpret_cast<int*>(c + 3 * n + 1);
+  launch_decide_batch(db, rounds, s);
+  BCK(cudaGetLastError());
+  int64_t launches = 2 * rounds;
+  BCK(cudaMemcpyAsync(c0.data(), c, c0.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+  BCK(cudaStreamSynchronize(s));
+  if (c0[3 * n + 1] != 0) {
+    cleanup();
+    return bfail(bt, ICAM_ERR_ROOM, "box list overflow");
+  }
+  std::vector<int64_t> off(n + 1, 0), n_read(n);
+  for (int i = 0; i < n; i++) {
+    n_read[i] = int64_t(c0[2 * n + i]);
+    if (n_read[i] > lvl_off[i + 1] - lvl_off[i]) {
+      cleanup();
+      return bfail(bt, ICAM_ERR_ROOM, "read list overflow");
+    }
+    off[i + 1] = off[i] + n_read[i];
+  }
+  const int64_t boxes_n = int64_t(c0[3 * n]);
   const int64_t R = off[n];
   const size_t Rb = size_t(std::max<int64_t>(R, 1));
   // the batch's arrays: first nodes, centre distances, brick indices and parts, words,
   // kinds, stored flags and slots, scan room, the atlas (room for every brick stored, so
   // that the whole of what follows can be one graph), part offsets and map pointers
-  void *firsts, *dcs, *idx, *part_of, *words, *kind, *flags, *tmp, *atlas, *d_off, *d_maps, *d_pslot;
-  size_t tmp_bytes = 0;
+  void *firsts, *dcs, *idx, *part_of, *words, *kind, *flags, *tmp, *atlas, *d_off, *d_maps, *d_pslot, *stmp;
+  size_t tmp_bytes = 0, sort_bytes = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, (int64_t*)nullptr, (int64_t*)nullptr, R + 1, s);
-  int r;
+  int end_bit = PART_SHIFT;
+  while ((int64_t(1) << (end_bit - PART_SHIFT)) < n) end_bit++;
+  cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, (uint64_t*)nullptr, (uint64_t*)nullptr, (double*)nullptr,
+                                  (double*)nullptr, R, 0, end_bit, s);
   if ((r = bbuf(bt, 0, Rb * 3 * sizeof(double), &firsts)) || (r = bbuf(bt, 1, Rb * sizeof(double), &dcs)) ||
       (r = bbuf(bt, 2, Rb * sizeof(int64_t), &idx)) || (r = bbuf(bt, 3, Rb * sizeof(int32_t), &part_of)) ||
       (r = bbuf(bt, 4, Rb * 365 * sizeof(uint32_t), &words)) || (r = bbuf(bt, 5, Rb * sizeof(int32_t), &kind)) ||
       (r = bbuf(bt, 6, (Rb + 1) * 2 * sizeof(int64_t), &flags)) || (r = bbuf(bt, 7, tmp_bytes + 16, &tmp)) ||
       (r = bbuf(bt, 8, Rb * 365 * sizeof(uint32_t), &atlas)) || (r = bbuf(bt, 9, (n + 1) * sizeof(int64_t), &d_off)) ||
-      (r = bbuf(bt, 10, n * sizeof(uint32_t*), &d_maps)) || (r = bbuf(bt, 11, (n + 1) * sizeof(int64_t), &d_pslot))) {
+      (r = bbuf(bt, 10, n * sizeof(uint32_t*), &d_maps)) || (r = bbuf(bt, 11, (n + 1) * sizeof(int64_t), &d_pslot)) ||
+      (r = bbuf(bt, 21, Rb * sizeof(uint64_t), &keys[0])) || (r = bbuf(bt, 22, Rb * sizeof(uint64_t), &keys[1])) ||
+      (r = bbuf(bt, 23, sort_bytes + 16, &stmp))) {
     cleanup();
     return r;
   }
   int64_t* slot = static_cast<int64_t*>(flags) + (Rb + 1);
+  BCK(cudaMemcpyAsync(d_off, off.data(), (n + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+  if (R > 0) {
+    // the read bricks of all parts in (part, brick) order: each part's in brick order
+    // (partcache.rs:486), the parts one after another
+    // gathered dense into keys[0] and dcs, the distances then moved to the read lists'
+    // room (free once gathered, and at least as long) as the sort's input
+    double* dc_tmp = static_cast<double*>(rdc);
+    k_batch_keys<<<grid_of(R, 256), 256, 0, s>>>(static_cast<const int64_t*>(ridx), static_cast<const double*>(rdc),
+                                                  static_cast<const int64_t*>(d_roff), static_cast<const int64_t*>(d_off),
+                                                  n, R, static_cast<uint64_t*>(keys[0]), static_cast<double*>(dcs));
+    BCK(cudaMemcpyAsync(dc_tmp, dcs, R * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    BCK(cub::DeviceRadixSort::SortPairs(stmp, sort_bytes, static_cast<const uint64_t*>(keys[0]),
+                                        static_cast<uint64_t*>(keys[1]), static_cast<const double*>(dc_tmp),
+                                        static_cast<double*>(dcs), R, 0, end_bit, s));
+    k_batch_split<<<grid_of(R, 256), 256, 0, s>>>(static_cast<const uint64_t*>(keys[1]), R,
+                                                   static_cast<const DecideArgs*>(d_args), static_cast<int64_t*>(idx),
+                                                   static_cast<int32_t*>(part_of), static_cast<double*>(firsts));
+    launches += 4;
+  }
+  BCK(cudaEventRecord(ev[1], s));
   std::vector<PartParams> hp(n);
-  std::vector<uint32_t*> maps(n);
   for (int i = 0; i < n; i++) {
     IcamPack* pk = bt->packs[i];
     const IcamBatchLevel& lv = levels[i];
-    const int64_t Ri = D[i].n_read;
-    if (Ri > 0) {
-      k_gather_firsts<<<grid_of(Ri, 256), 256, 0, s>>>(D[i].read_idx, Ri, lv.nb[0], lv.nb[1], lv.h, lv.lo[0], lv.lo[1],
-                                                      lv.lo[2], static_cast<double*>(firsts) + 3 * off[i]);
-      k_fill_part<<<grid_of(Ri, 256), 256, 0, s>>>(static_cast<int32_t*>(part_of) + off[i], Ri, i);
-      BCK(cudaMemcpyAsync(static_cast<double*>(dcs) + off[i], D[i].read_dc, Ri * sizeof(double),
-                          cudaMemcpyDeviceToDevice, s));
-      BCK(cudaMemcpyAsync(static_cast<int64_t*>(idx) + off[i], D[i].read_idx, Ri * sizeof(int64_t),
-                          cudaMemcpyDeviceToDevice, s));
-      launches += 2;
-    }
     PartParams& q = hp[i];
     std::memset(&q, 0, sizeof(q));
     q.P = pk->dev;
@@ -259,10 +385,8 @@ int icam_batch_bake(IcamBatch* bt, const IcamBatchLevel* levels, int precision, 
     q.h = lv.h;
     q.clamp = lv.clamp;
     if (precision == ICAM_MIXED_LEARNED) q.net_feat = pk->net.feat, q.net_w = pk->net.wbf;
-    maps[i] = D[i].map;
   }
   BCK(cudaMemcpyAsync(bt->d_parts, hp.data(), n * sizeof(PartParams), cudaMemcpyHostToDevice, s));
-  BCK(cudaMemcpyAsync(d_off, off.data(), (n + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
   BCK(cudaMemcpyAsync(d_maps, maps.data(), n * sizeof(uint32_t*), cudaMemcpyHostToDevice, s));
   BrickArgs a{};
   a.parts = bt->d_parts;
@@ -340,12 +464,12 @@ int icam_batch_bake(IcamBatch* bt, const IcamBatchLevel* levels, int precision, 
     parts_out[i].d_map = maps[i];
     parts_out[i].d_atlas = static_cast<const uint32_t*>(atlas) + size_t(pslot[i]) * 365;
     parts_out[i].n_slots = size_t(pslot[i + 1] - pslot[i]);
-    parts_out[i].bricks_read = D[i].n_read;
+    parts_out[i].bricks_read = n_read[i];
   }
   if (stats) {
     std::memset(stats, 0, sizeof(*stats));
     stats->parts = n;
-    stats->boxes_read = boxes;
+    stats->boxes_read = boxes_n;
     stats->bricks_read = R;
     stats->bricks_words = pslot[n];
     stats->nodes_exact = int64_t(st[0]);

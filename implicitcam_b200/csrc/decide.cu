@@ -26,7 +26,8 @@ static_assert(sizeof(DecideSmem) * DWARPS <= 48 * 1024, "static shared memory of
 // One box's verdict from its centre's value (v, f) read within `cut` (partcache.rs:370-383:
 // decided once the centre is known past the box grown by the clamp), the map entries it
 // settles, and its children (8 to a box, appended together) or its read.
-__device__ void decide_box(const DecideArgs& a, const Box4& b, double3 c, double r, double cut, double v, int f) {
+__device__ void decide_box(const DecideArgs& a, long long size, const Box4& b, double3 c, double r, double cut,
+                           double v, int f) {
   const DPack& P = a.P;
   const double side = 8.0 * a.h;
   double sd = NAN;  // the signed distance at the centre when known
@@ -54,10 +55,10 @@ __device__ void decide_box(const DecideArgs& a, const Box4& b, double3 c, double
   const long long nb0 = a.nb[0], nb1 = a.nb[1], nb2 = a.nb[2];
   if (verdict != 0) {
     uint32_t val = verdict == 1 ? 0xffffffffu : 0xfffffffeu;
-    for (long long z = max(b.z, 0LL); z < min(b.z + a.size, nb2); z++)
-      for (long long y = max(b.y, 0LL); y < min(b.y + a.size, nb1); y++)
-        for (long long x = max(b.x, 0LL); x < min(b.x + a.size, nb0); x++) a.map[x + nb0 * (y + nb1 * z)] = val;
-  } else if (a.size == 1) {
+    for (long long z = max(b.z, 0LL); z < min(b.z + size, nb2); z++)
+      for (long long y = max(b.y, 0LL); y < min(b.y + size, nb1); y++)
+        for (long long x = max(b.x, 0LL); x < min(b.x + size, nb0); x++) a.map[x + nb0 * (y + nb1 * z)] = val;
+  } else if (size == 1) {
     long long idx = b.x + nb0 * (b.y + nb1 * b.z);
     a.map[idx] = 0xfffffff0u;  // read
     unsigned long long slot = atomicAdd(a.n_read, 1ull);
@@ -66,7 +67,7 @@ __device__ void decide_box(const DecideArgs& a, const Box4& b, double3 c, double
       a.read_dc[slot] = sd;
     }
   } else {
-    const long long half = a.size / 2;
+    const long long half = size / 2;
     Box4 kids[8];
     int nk = 0;
     for (int q = 0; q < 8; q++) {
@@ -89,63 +90,108 @@ __device__ void decide_box(const DecideArgs& a, const Box4& b, double3 c, double
   }
 }
 
-// 32 boxes a warp: their centres' bounding ball, the features within its radius plus the
-// cut of its centre (listed and ranked once, sub-patches seeded there), every centre's
-// value capped at the cut by the shared walk, then each box decided.
+// 32 boxes of one size from boxes[g0 ..] (n in all): their centres' bounding ball, the
+// features within its radius plus the cut of its centre (listed and ranked once,
+// sub-patches seeded there), every centre's value capped at the cut by the shared walk,
+// then each box decided.
+__device__ __forceinline__ void decide_group(const DecideArgs& a, const Box4* boxes, int64_t n, long long size,
+                                             int64_t g0, DecideSmem& S, int lane) {
+  const DPack& P = a.P;
+  const double side = 8.0 * a.h;
+  const int64_t i = g0 + lane;
+  const bool live = i < n;
+  const Box4 b = boxes[live ? i : g0];
+  double3 lo = mk(a.lo[0] + side * b.x - a.clamp, a.lo[1] + side * b.y - a.clamp, a.lo[2] + side * b.z - a.clamp);
+  double3 hi = mk(a.lo[0] + side * (b.x + size) + a.clamp, a.lo[1] + side * (b.y + size) + a.clamp,
+                  a.lo[2] + side * (b.z + size) + a.clamp);
+  const double3 c = (lo + hi) * 0.5;
+  const double r = 0.5 * len(hi - lo);
+  const double cut = (r + a.clamp) * (1.0 + 1e-4);
+  // the group's centre: the middle of its centres' box; its radius, the farthest centre
+  double bl[3] = {c.x, c.y, c.z}, bh[3] = {c.x, c.y, c.z};
+  for (int o = 16; o > 0; o >>= 1)
+    for (int k = 0; k < 3; k++) {
+      bl[k] = fmin(bl[k], __shfl_xor_sync(FULL, bl[k], o));
+      bh[k] = fmax(bh[k], __shfl_xor_sync(FULL, bh[k], o));
+    }
+  const double3 gc = mk(0.5 * (bl[0] + bh[0]), 0.5 * (bl[1] + bh[1]), 0.5 * (bl[2] + bh[2]));
+  double R = len(c - gc);
+  for (int o = 16; o > 0; o >>= 1) R = fmax(R, __shfl_xor_sync(FULL, R, o));
+  // every feature nearer than the cut to a centre has a bound <= R + cut from gc
+  int nc = warp_list(P, a.leaves, a.n_leaves, gc, R + cut, S.tcode, S.tlb, S.fr, &S.n, lane);
+  const bool overflow = nc > MAXC;
+  if (overflow) nc = MAXC;
+  warp_rank(S.tcode, S.tlb, nc, S.code, S.lb, lane);
+  int subs_before = 0;
+  for (int base = 0; base < nc; base += 32) {
+    const int k = base + lane;
+    const bool is_sub = k < nc && (S.code[k] >> IK_SHIFT) == IK_SUB;
+    const unsigned m = __ballot_sync(FULL, is_sub);
+    const int before = subs_before + __popc(m & ((1u << lane) - 1u));
+    subs_before += __popc(m);
+    if (k >= nc) continue;
+    int slot = -1;
+    if (is_sub && before < MAXSUB) {
+      slot = before;
+      S.seed[slot] = seed_at(P.sub_cp + 16 * size_t(S.code[k] & IK_MASK), gc);
+    }
+    S.cert[k] = 0;
+    S.slot[k] = int8_t(slot);
+  }
+  __syncwarp();
+  const WarpCands W{S.code, S.lb, S.cert, S.slot, S.seed, S.net, S.net32, nc, overflow};
+  double v;
+  int f;
+  warp_point<false>(P, W, c, gc, live, cut, lane, &v, &f);
+  if (live) decide_box(a, size, b, c, r, cut, v, f);
+  __syncwarp();
+}
+
 __global__ void __launch_bounds__(DWARPS * 32, 2) k_decide_w(DecideArgs a) {
   __shared__ DecideSmem smem[DWARPS];
-  const DPack& P = a.P;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  DecideSmem& S = smem[warp];
-  const double side = 8.0 * a.h;
-  for (int64_t g0 = (int64_t(blockIdx.x) * DWARPS + warp) * 32; g0 < a.n; g0 += int64_t(gridDim.x) * DWARPS * 32) {
-    const int64_t i = g0 + lane;
-    const bool live = i < a.n;
-    const Box4 b = a.boxes[live ? i : g0];
-    double3 lo = mk(a.lo[0] + side * b.x - a.clamp, a.lo[1] + side * b.y - a.clamp, a.lo[2] + side * b.z - a.clamp);
-    double3 hi = mk(a.lo[0] + side * (b.x + a.size) + a.clamp, a.lo[1] + side * (b.y + a.size) + a.clamp,
-                    a.lo[2] + side * (b.z + a.size) + a.clamp);
-    const double3 c = (lo + hi) * 0.5;
-    const double r = 0.5 * len(hi - lo);
-    const double cut = (r + a.clamp) * (1.0 + 1e-4);
-    // the group's centre: the middle of its centres' box; its radius, the farthest centre
-    double bl[3] = {c.x, c.y, c.z}, bh[3] = {c.x, c.y, c.z};
-    for (int o = 16; o > 0; o >>= 1)
-      for (int k = 0; k < 3; k++) {
-        bl[k] = fmin(bl[k], __shfl_xor_sync(FULL, bl[k], o));
-        bh[k] = fmax(bh[k], __shfl_xor_sync(FULL, bh[k], o));
-      }
-    const double3 gc = mk(0.5 * (bl[0] + bh[0]), 0.5 * (bl[1] + bh[1]), 0.5 * (bl[2] + bh[2]));
-    double R = len(c - gc);
-    for (int o = 16; o > 0; o >>= 1) R = fmax(R, __shfl_xor_sync(FULL, R, o));
-    // every feature nearer than the cut to a centre has a bound <= R + cut from gc
-    int n = warp_list(P, a.leaves, a.n_leaves, gc, R + cut, S.tcode, S.tlb, S.fr, &S.n, lane);
-    const bool overflow = n > MAXC;
-    if (overflow) n = MAXC;
-    warp_rank(S.tcode, S.tlb, n, S.code, S.lb, lane);
-    int subs_before = 0;
-    for (int base = 0; base < n; base += 32) {
-      const int k = base + lane;
-      const bool is_sub = k < n && (S.code[k] >> IK_SHIFT) == IK_SUB;
-      const unsigned m = __ballot_sync(FULL, is_sub);
-      const int before = subs_before + __popc(m & ((1u << lane) - 1u));
-      subs_before += __popc(m);
-      if (k >= n) continue;
-      int slot = -1;
-      if (is_sub && before < MAXSUB) {
-        slot = before;
-        S.seed[slot] = seed_at(P.sub_cp + 16 * size_t(S.code[k] & IK_MASK), gc);
-      }
-      S.cert[k] = 0;
-      S.slot[k] = int8_t(slot);
+  for (int64_t g0 = (int64_t(blockIdx.x) * DWARPS + warp) * 32; g0 < a.n; g0 += int64_t(gridDim.x) * DWARPS * 32)
+    decide_group(a, a.boxes, a.n, a.size, g0, smem[warp], lane);
+}
+
+// A batch's round (one box size a part): the counts the last round appended become this
+// round's, the next counts start at zero, and the parts' groups of 32 are numbered.
+// One thread: a batch holds tens to thousands of parts.
+__global__ void k_decide_prep(DecideBatchArgs b, int round) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  int64_t g = 0;
+  for (int p = 0; p < b.n_parts; p++) {
+    unsigned long long* cur = b.cnt + 2 * p + (round & 1);
+    unsigned long long* next = b.cnt + 2 * p + ((round + 1) & 1);
+    const DecideArgs& a = b.args[2 * p + (round & 1)];
+    if (*cur > (unsigned long long)a.next_cap) {
+      *b.err = 1;
+      *cur = (unsigned long long)a.next_cap;
     }
-    __syncwarp();
-    const WarpCands W{S.code, S.lb, S.cert, S.slot, S.seed, S.net, S.net32, n, overflow};
-    double v;
-    int f;
-    warp_point<false>(P, W, c, gc, live, cut, lane, &v, &f);
-    if (live) decide_box(a, b, c, r, cut, v, f);
-    __syncwarp();
+    *next = 0;
+    b.boxes_read[0] += *cur;
+    b.groups[p] = g;
+    g += int64_t((*cur + 31) / 32);
+  }
+  b.groups[b.n_parts] = g;
+}
+
+// A batch's round: every part's boxes of this round's size, 32 of one part a warp, the
+// warps taking groups across all parts from the numbering k_decide_prep made.
+__global__ void __launch_bounds__(DWARPS * 32, 2) k_decide_batch(DecideBatchArgs b, int round) {
+  __shared__ DecideSmem smem[DWARPS];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t total = b.groups[b.n_parts];
+  for (int64_t g = int64_t(blockIdx.x) * DWARPS + warp; g < total; g += int64_t(gridDim.x) * DWARPS) {
+    int lo = 0, hi = b.n_parts;  // the part: groups[p] <= g < groups[p + 1]
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) / 2;
+      if (b.groups[mid] <= g) lo = mid;
+      else hi = mid;
+    }
+    const DecideArgs& a = b.args[2 * lo + (round & 1)];
+    const int64_t n = int64_t(b.cnt[2 * lo + (round & 1)]);
+    decide_group(a, a.boxes, n, a.size >> round, (g - b.groups[lo]) * 32, smem[warp], lane);
   }
 }
 
@@ -155,6 +201,15 @@ void launch_decide(const DecideArgs& a, cudaStream_t s) {
   const int64_t want = (a.n + DWARPS * 32 - 1) / (DWARPS * 32);
   const int grid = int(std::max<int64_t>(1, std::min<int64_t>(want, int64_t(sms) * 2)));
   k_decide_w<<<grid, DWARPS * 32, 0, s>>>(a);
+}
+
+void launch_decide_batch(const DecideBatchArgs& b, int rounds, cudaStream_t s) {
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  for (int r = 0; r < rounds; r++) {
+    k_decide_prep<<<1, 32, 0, s>>>(b, r);
+    k_decide_batch<<<sms * 2, DWARPS * 32, 0, s>>>(b, r);
+  }
 }
 
 }  // namespace icam

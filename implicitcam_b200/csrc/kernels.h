@@ -83,6 +83,22 @@ __global__ void k_assemble_batch(const int64_t* idx, const int32_t* part_of, con
                                  const uint32_t* words, uint32_t* atlas);
 // The decision of one box size of a level (decide.cu), 32 boxes a warp.
 void launch_decide(const DecideArgs& a, cudaStream_t s);
+
+// Many parts' decisions together (decide.cu), one round a box size. Part p's fields are
+// args[2p + (round & 1)]: `size` its first boxes' size (round r decides size >> r),
+// boxes / next its two box regions (swapped between the pair), n_next its next count
+// (cnt[2p + ((round + 1) & 1)]), n_read its read count. cnt[2p] holds the first boxes'
+// count at the start; groups (n_parts + 1 values) is k_decide_prep's numbering.
+struct DecideBatchArgs {
+  const DecideArgs* args;
+  int n_parts;
+  unsigned long long* cnt;
+  int64_t* groups;
+  unsigned long long* boxes_read;
+  int* err;  // set when a part's box list would overflow
+};
+// `rounds` rounds (the largest first box size's log2 + 1), no host synchronisation.
+void launch_decide_batch(const DecideBatchArgs& b, int rounds, cudaStream_t s);
 __global__ void k_gather_firsts(const int64_t* idx, int64_t n, int64_t nb0, int64_t nb1, double h, double lo0,
                                 double lo1, double lo2, double* firsts);
 __global__ void k_assemble(const int64_t* idx, const int32_t* kind, const int64_t* slot, int64_t n,

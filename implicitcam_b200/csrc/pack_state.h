@@ -47,6 +47,12 @@ struct DecideOut {
   int64_t n_read = 0, boxes_read = 0, launches = 0;
 };
 
+namespace icam {
+struct Box4;
+}
+// api.cu: the first boxes of a level's decision (their size in bricks returned).
+long long first_boxes(const LevelDesc& L, std::vector<icam::Box4>* out);
+
 struct IcamPack;
 // api.cu: the decision (partcache.rs:226-331) through the sort of the read bricks.
 int decide_level(IcamPack* pk, const LevelDesc& L, DecideOut* out);

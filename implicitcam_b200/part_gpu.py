@@ -304,9 +304,10 @@ def unpack_atlas(atlas):
 
 
 class Batch:
-    """Many parts baked together (icam_batch_*, include/icam_cuda.h): each part's box
-    decision on its own pack, then all parts' bricks in one launch of the brick kernel,
-    the rest replayed as a CUDA graph. No counterpart in the reference."""
+    """Many parts baked together (icam_batch_*, include/icam_cuda.h): all parts' box
+    decisions in one launch a box size, all parts' bricks in one launch of the brick
+    kernel, the rest replayed as a CUDA graph. A part may appear more than once (e.g. at
+    two resolutions). No counterpart in the reference."""
 
     def __init__(self, parts):
         self.parts = list(parts)

@@ -10,7 +10,10 @@
   rational B-spline with 16 x 16 control points, heights 50 mm plus 8 seeded
   Gaussian bumps, weights in [0.8, 1.2];
 - ``frustum``, ``ball``, ``ring``: a cone-sided can, a sphere and a torus, the analytic
-  surface kinds the parts above lack (the sphere and torus have no edges at all).
+  surface kinds the parts above lack (the sphere and torus have no edges at all);
+- ``boss`` (cylinder, torus fillet, plane cap), ``countersunk_block`` (a hole with a
+  cone countersink) and ``dome`` (a cylinder under a hemisphere): the analytic families
+  of a batch of uneven parts.
 
 Random numbers come from the reference checkers' xorshift64 generator
 (crates/icam-check/src/exact_check.rs:45-52) seeded through splitmix64, so that
@@ -333,6 +336,127 @@ def ring(major=4.0, minor=1.5):
     b = SolidBuilder(tol=1e-9)
     b.face(TORUS, +1, Frame([0, 0, 0], [0, 0, 1], [1, 0, 0]), a=major, b=minor, lo=[0.0, -math.pi],
            hi=[TAU, math.pi], period=[TAU, TAU])
+    return b
+
+
+def boss(r=3.0, height=5.0, fillet=1.0):
+    """A boss: the can with its top edge rounded by a quarter-torus fillet (bottom plane,
+    cylinder to height - fillet, torus of major r - fillet and minor fillet, top plane
+    of radius r - fillet; three circles, two seams)."""
+    b = SolidBuilder(tol=1e-9)
+    z, x = [0, 0, 1], [1, 0, 0]
+    zm = height - fillet
+    f0, fm, f1 = Frame([0, 0, 0], z, x), Frame([0, 0, zm], z, x), Frame([0, 0, height], z, x)
+    va, vm, vt = b.vertex([r, 0, 0]), b.vertex([r, 0, zm]), b.vertex([r - fillet, 0, height])
+    c0 = b.arc(f0, r, 0.0, TAU, va, va)
+    cm = b.arc(fm, r, 0.0, TAU, vm, vm)
+    ct = b.arc(f1, r - fillet, 0.0, TAU, vt, vt)
+    seam_c = b.line(va, vm)
+    # the fillet's seam: a quarter circle in the xz plane from (r, 0, zm) up to (r - f, 0, h)
+    seam_t = b.arc(Frame([r - fillet, 0, zm], [0, -1, 0], [1, 0, 0]), fillet, 0.0, math.pi / 2, vm, vt)
+    _plane_face(b, f0, -1, [[(c0, True)]])
+    _plane_face(b, f1, +1, [[(ct, False)]])
+    lo, hi = _pad([0.0, 0.0], [TAU, zm])
+    cyl = b.face(CYLINDER, +1, f0, a=r, lo=[0.0, lo[1]], hi=[TAU, hi[1]], period=[TAU, 0.0])
+    b.loop(cyl, [
+        (c0, False, line_pcurve([0.0, 0.0], [TAU, 0.0])),
+        (seam_c, False, None),
+        (cm, True, line_pcurve([TAU, zm], [0.0, zm])),
+        (seam_c, True, None),
+    ])
+    lo, hi = _pad([0.0, 0.0], [TAU, math.pi / 2])
+    tor = b.face(TORUS, +1, fm, a=r - fillet, b=fillet, lo=[0.0, lo[1]], hi=[TAU, hi[1]], period=[TAU, 0.0])
+    b.loop(tor, [
+        (cm, False, line_pcurve([0.0, 0.0], [TAU, 0.0])),
+        (seam_t, False, None),
+        (ct, True, line_pcurve([TAU, math.pi / 2], [0.0, math.pi / 2])),
+        (seam_t, True, None),
+    ])
+    return b
+
+
+def dome(r=3.0, height=4.0):
+    """A spherical dome: a cylinder of radius r to `height` capped by the hemisphere on
+    its top circle (bottom plane, cylinder, sphere; two circles, one seam). The sphere's
+    one loop is its equator; its pole lies inside the face."""
+    b = SolidBuilder(tol=1e-9)
+    z, x = [0, 0, 1], [1, 0, 0]
+    f0, f1 = Frame([0, 0, 0], z, x), Frame([0, 0, height], z, x)
+    va, vb = b.vertex([r, 0, 0]), b.vertex([r, 0, height])
+    c0 = b.arc(f0, r, 0.0, TAU, va, va)
+    c1 = b.arc(f1, r, 0.0, TAU, vb, vb)
+    seam = b.line(va, vb)
+    _plane_face(b, f0, -1, [[(c0, True)]])
+    lo, hi = _pad([0.0, 0.0], [TAU, height])
+    cyl = b.face(CYLINDER, +1, f0, a=r, lo=[0.0, lo[1]], hi=[TAU, hi[1]], period=[TAU, 0.0])
+    b.loop(cyl, [
+        (c0, False, line_pcurve([0.0, 0.0], [TAU, 0.0])),
+        (seam, False, None),
+        (c1, True, line_pcurve([TAU, height], [0.0, height])),
+        (seam, True, None),
+    ])
+    lo, hi = _pad([0.0, 0.0], [TAU, math.pi / 2])
+    sph = b.face(SPHERE, +1, f1, a=r, lo=[0.0, lo[1]], hi=[TAU, hi[1]], period=[TAU, 0.0])
+    b.loop(sph, [(c1, False, line_pcurve([0.0, 0.0], [TAU, 0.0]))])
+    return b
+
+
+def countersunk_block(size=(40.0, 30.0, 20.0), center=(20.0, 15.0), r=4.0, sink=2.0, half_angle_deg=45.0):
+    """A block [0,X]x[0,Y]x[0,Z] with a through-hole of radius r along z whose top
+    `sink` mm widens as a cone (the countersink) to r + sink tan(angle) at z = Z."""
+    X, Y, Z = size
+    ang = math.radians(half_angle_deg)
+    rt = r + sink * math.tan(ang)
+    zm = Z - sink
+    b = SolidBuilder(tol=1e-9)
+    c = {}
+    for i, xx in enumerate((0.0, X)):
+        for j, yy in enumerate((0.0, Y)):
+            for k, zz in enumerate((0.0, Z)):
+                c[i, j, k] = b.vertex([xx, yy, zz])
+    L = lambda p, q: b.line(c[p], c[q])  # noqa: E731
+    eb = [L((0, 0, 0), (1, 0, 0)), L((1, 0, 0), (1, 1, 0)), L((1, 1, 0), (0, 1, 0)), L((0, 1, 0), (0, 0, 0))]
+    et = [L((0, 0, 1), (1, 0, 1)), L((1, 0, 1), (1, 1, 1)), L((1, 1, 1), (0, 1, 1)), L((0, 1, 1), (0, 0, 1))]
+    ev = {ij: L((*ij, 0), (*ij, 1)) for ij in ((0, 0), (1, 0), (1, 1), (0, 1))}
+    cx, cy = center
+    va, vm, vb = b.vertex([cx + r, cy, 0.0]), b.vertex([cx + r, cy, zm]), b.vertex([cx + rt, cy, Z])
+    fz0 = Frame([cx, cy, 0.0], [0, 0, 1], [1, 0, 0])
+    fzm = Frame([cx, cy, zm], [0, 0, 1], [1, 0, 0])
+    fz1 = Frame([cx, cy, Z], [0, 0, 1], [1, 0, 0])
+    c0 = b.arc(fz0, r, 0.0, TAU, va, va)
+    cm = b.arc(fzm, r, 0.0, TAU, vm, vm)
+    c1 = b.arc(fz1, rt, 0.0, TAU, vb, vb)
+    seam_c = b.line(va, vm)
+    seam_k = b.line(vm, vb)
+    _plane_face(b, Frame([0, 0, 0], [0, 0, 1], [1, 0, 0]), -1,
+                [[(eb[3], True), (eb[2], True), (eb[1], True), (eb[0], True)], [(c0, False)]])
+    _plane_face(b, Frame([0, 0, Z], [0, 0, 1], [1, 0, 0]), +1,
+                [[(et[0], False), (et[1], False), (et[2], False), (et[3], False)], [(c1, True)]])
+    _plane_face(b, Frame([0, 0, 0], [0, -1, 0], [1, 0, 0]), +1,
+                [[(eb[0], False), (ev[1, 0], False), (et[0], True), (ev[0, 0], True)]])
+    _plane_face(b, Frame([X, 0, 0], [1, 0, 0], [0, 1, 0]), +1,
+                [[(eb[1], False), (ev[1, 1], False), (et[1], True), (ev[1, 0], True)]])
+    _plane_face(b, Frame([X, Y, 0], [0, 1, 0], [-1, 0, 0]), +1,
+                [[(eb[2], False), (ev[0, 1], False), (et[2], True), (ev[1, 1], True)]])
+    _plane_face(b, Frame([0, Y, 0], [-1, 0, 0], [0, -1, 0]), +1,
+                [[(eb[3], False), (ev[0, 0], False), (et[3], True), (ev[0, 1], True)]])
+    # the hole's wall and the countersink: outward toward the axis (sense -1)
+    lo, hi = _pad([0.0, 0.0], [TAU, zm])
+    cyl = b.face(CYLINDER, -1, fz0, a=r, lo=[0.0, lo[1]], hi=[TAU, hi[1]], period=[TAU, 0.0])
+    b.loop(cyl, [
+        (cm, False, line_pcurve([0.0, zm], [TAU, zm])),
+        (seam_c, True, None),
+        (c0, True, line_pcurve([TAU, 0.0], [0.0, 0.0])),
+        (seam_c, False, None),
+    ])
+    lo, hi = _pad([0.0, 0.0], [TAU, sink])
+    cone = b.face(CONE, -1, fzm, a=r, b=ang, lo=[0.0, lo[1]], hi=[TAU, hi[1]], period=[TAU, 0.0])
+    b.loop(cone, [
+        (c1, False, line_pcurve([0.0, sink], [TAU, sink])),
+        (seam_k, True, None),
+        (cm, True, line_pcurve([TAU, 0.0], [0.0, 0.0])),
+        (seam_k, False, None),
+    ])
     return b
 
 

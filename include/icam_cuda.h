@@ -187,7 +187,7 @@ typedef struct IcamBatchLevel { /* one part's level, as icam_bake_level takes it
 } IcamBatchLevel;
 
 typedef struct IcamBatchPart { /* one part's level, in device memory */
-  const uint32_t* d_map;       /* nb[0] x nb[1] x nb[2] entries (in the part's pack) */
+  const uint32_t* d_map;       /* nb[0] x nb[1] x nb[2] entries (in the batch) */
   const uint32_t* d_atlas;     /* n_slots x 365 words (in the batch) */
   size_t n_slots;
   int64_t bricks_read;
@@ -202,12 +202,13 @@ typedef struct IcamBatchStats {
   double ms_decide, ms_bricks;
 } IcamBatchStats;
 
-/* A batch over n packs (distinct, one device). The packs must outlive it, and no other
- * call may use them while a batch bake runs (their scratch holds its decisions). */
+/* A batch over n packs on one device (a pack may appear more than once, e.g. to bake one
+ * part at two resolutions). The packs must outlive it; a pack's own calls and a batch
+ * bake that uses it must not run at the same time. */
 int icam_batch_create(IcamPack* const* packs, size_t n, IcamBatch** out, char* err, size_t errlen);
 void icam_batch_destroy(IcamBatch* batch);
 /* Bakes levels[i] of part i, all parts together; parts_out[i] its results, valid until
- * the next bake of the batch or of the part's pack. */
+ * the next bake of the batch. */
 int icam_batch_bake(IcamBatch* batch, const IcamBatchLevel* levels, int precision, IcamBatchPart* parts_out,
                     IcamBatchStats* stats);
 const char* icam_batch_last_error(const IcamBatch* batch);

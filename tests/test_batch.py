@@ -1,6 +1,7 @@
 """Batches (icam_batch_*): uneven parts baked together give every part the map and atlas
 of baking it alone, bit for bit (FP64) and in the mixed form; a second bake of the same
-levels replays the captured graph; the tiling is one the autotuner timed."""
+levels replays the captured graph; the tiling is one the autotuner timed; one part may
+be baked at two resolutions in one batch; a bad level is refused."""
 import numpy as np
 import pytest
 
@@ -64,7 +65,29 @@ def test_batch_equals_parts_alone(batch, precision):
         assert np.array_equal(m, m2) and np.array_equal(a, a2)
 
 
-def test_a_pack_twice_is_refused(batch):
+def test_one_part_at_two_resolutions(batch):
+    """The same pack twice in a batch, at two cell sizes: each level as baked alone."""
+    b0, gs, levels = batch
+    g = gs[1]
+    h, lo, nb, clamp = levels[1]
+    two = [(h, lo, nb, clamp), (h / 2, lo, 2 * nb, clamp / 2)]
+    b = part_gpu.Batch([g, g])
+    try:
+        st, res = b.bake(two)
+        assert st["parts"] == 2 and st["nodes_undecided"] == 0
+        for L, (m, a) in zip(two, res):
+            m1, a1, _ = g.level(*L)
+            assert np.array_equal(m, m1) and np.array_equal(a, a1)
+    finally:
+        b.close()
+
+
+def test_bad_levels_are_refused(batch):
     b, gs, levels = batch
+    bad = list(levels)
+    h, lo, nb, clamp = bad[2]
+    bad[2] = (h, lo, np.array([nb[0], 0, nb[2]]), clamp)
     with pytest.raises(part_gpu.IcamError):
-        part_gpu.Batch([gs[0], gs[0]])
+        b.bake(bad)
+    st, _ = b.bake(levels)  # the batch still bakes
+    assert st["parts"] == len(gs)
