@@ -55,19 +55,33 @@ def set_level(h, band):
     H, BAND = h, band
 
 
-def workload(seed: int):
+def workload(seed: int, kind: str = "freeform"):
+    """The part and its level's (lo, nb): the freeform top's whole box, or the mold
+    cavity's pocket (its floor of 500 B-spline faces and the walls' lower parts)."""
     from implicitcam_b200 import parts
 
-    b = parts.freeform_top(seed=seed)
-    # the part's box: the control net's box (the top is within its control points)
-    pts = np.asarray(b.verts)
-    net = np.concatenate([np.asarray(p).reshape(-1, 4) for p in b.patches])
-    xyz = net[:, :3] / net[:, 3:]
-    lo = np.minimum(pts.min(0), xyz.min(0))
-    hi = np.maximum(pts.max(0), xyz.max(0))
+    if kind == "mold":
+        b = parts.mold(seed=seed)
+        net = np.concatenate([np.asarray(p).reshape(-1, 4) for p in b.patches])
+        xyz = net[:, :3] / net[:, 3:]  # the floor lies within its control points
+        lo, hi = xyz.min(0), xyz.max(0)
+    else:
+        b = parts.freeform_top(seed=seed)
+        # the part's box: the control net's box (the top is within its control points)
+        pts = np.asarray(b.verts)
+        net = np.concatenate([np.asarray(p).reshape(-1, 4) for p in b.patches])
+        xyz = net[:, :3] / net[:, 3:]
+        lo = np.minimum(pts.min(0), xyz.min(0))
+        hi = np.maximum(pts.max(0), xyz.max(0))
     lo = lo - BAND
     nb = np.ceil((hi + BAND - lo) / (8 * H)).astype(np.int64)
     return b, lo, nb
+
+
+def workload_name(kind):
+    if kind == "mold":
+        return f"mold cavity pocket level bake (500 B-spline floor faces), h={H} mm, band +-{BAND} mm"
+    return f"freeform-top level bake, h={H} mm, band +-{BAND} mm"
 
 
 def sample_clocks(path):
@@ -102,24 +116,24 @@ def read_clocks(path, device):
             "samples": len(sm)}
 
 
-def cpu_bake_sample(seed, bricks_target_s=12.0, threads=None):
+def cpu_bake_sample(seed, bricks_target_s=12.0, threads=None, kind="freeform"):
     """The oracle's bake (the reference's exact_brick, partcache.rs:979) of a sample of
     the level's read bricks on all host cores: voxels/s, cores, sample text."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import icam_oracle
 
-    b, lo, nb = workload(seed)
+    b, lo, nb = workload(seed, kind)
     o = icam_oracle.Oracle(b, threads=threads)
     rng = np.random.default_rng(seed)
-    # bricks the bake reads: those holding random points of the freeform top (every
+    # bricks the bake reads: those holding random points of the B-spline spans (every
     # brick the surface passes through is read)
-    pa = np.asarray(b.patches[0]).reshape(13, 13, 4, 4, 4)
+    pa = np.concatenate([np.asarray(p).reshape(-1, 4, 4, 4) for p in b.patches])
     k = 4096
-    ia, ib = rng.integers(0, 13, k), rng.integers(0, 13, k)
+    ia = rng.integers(0, len(pa), k)
     s, t = rng.uniform(0, 1, k), rng.uniform(0, 1, k)
     bs = np.stack([(1 - s) ** 3, 3 * (1 - s) ** 2 * s, 3 * (1 - s) * s * s, s ** 3], 1)
     bt = np.stack([(1 - t) ** 3, 3 * (1 - t) ** 2 * t, 3 * (1 - t) * t * t, t ** 3], 1)
-    hom = np.einsum("ki,kj,kijc->kc", bs, bt, pa[ia, ib])
+    hom = np.einsum("ki,kj,kijc->kc", bs, bt, pa[ia])
     xyz = hom[:, :3] / hom[:, 3:]
     cell = np.floor((xyz - lo) / (8 * H)).astype(np.int64)
     firsts = lo + 8 * H * np.unique(cell, axis=0)
@@ -132,7 +146,7 @@ def cpu_bake_sample(seed, bricks_target_s=12.0, threads=None):
     t0 = time.perf_counter()
     o.bricks(firsts[:n2], H, BAND)
     dt = time.perf_counter() - t0
-    return 512.0 * n2 / dt, o.threads, f"{n2} random read bricks of the top's window (h={H}, clamp={BAND}), {dt:.1f} s"
+    return 512.0 * n2 / dt, o.threads, f"{n2} random read bricks through the B-spline spans (h={H}, clamp={BAND}), {dt:.1f} s"
 
 
 def run_reference(args, rank, world):
@@ -140,16 +154,16 @@ def run_reference(args, rank, world):
         return
     vals = []
     for _ in range(args.warmup):
-        cpu_bake_sample(0, bricks_target_s=2.0)
+        cpu_bake_sample(0, bricks_target_s=2.0, kind=args.workload)
     for _ in range(args.steps):
-        v, cores, sample = cpu_bake_sample(0, bricks_target_s=8.0)
+        v, cores, sample = cpu_bake_sample(0, bricks_target_s=8.0, kind=args.workload)
         vals.append(v)
     value = float(np.mean(vals))
     out = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "voxels/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"freeform-top level bake, h={H} mm, band +-{BAND} mm", "seed": 0},
+        "config": {"workload": workload_name(args.workload), "seed": 0},
         "cpu_baseline": {"value": value, "unit": "voxels/s", "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "voxels/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -165,14 +179,16 @@ def main():
     ap.add_argument("--precision", default="learned", choices=["fp64", "mixed", "learned"],
                     help="the headline arm; the plain FP64 arm is timed beside it")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--h", type=float, default=H, help="cell side (mm); smaller cases for profiling")
-    ap.add_argument("--band", type=float, default=BAND, help="narrow band half-width (mm), the clamp")
-    ap.add_argument("--workload", default="freeform", choices=["freeform", "batch"],
-                    help="batch: 64 seeded uneven parts at h = 0.2 mm baked together (not the headline)")
+    ap.add_argument("--h", type=float, default=None, help="cell side (mm); smaller cases for profiling")
+    ap.add_argument("--band", type=float, default=None, help="narrow band half-width (mm), the clamp")
+    ap.add_argument("--workload", default="freeform", choices=["freeform", "batch", "mold"],
+                    help="freeform: the headline (h 0.1 mm, band 2 mm); mold: the mold cavity's pocket "
+                         "(h 0.05 mm, band 1 mm); batch: 64 seeded uneven parts at h = 0.2 mm baked together")
     ap.add_argument("--seednet-steps", type=int, default=SEEDNET_STEPS,
                     help="training steps of the seed network (fewer only for profiling captures)")
     args = ap.parse_args()
-    set_level(args.h, args.band)
+    dh, db = (0.05, 1.0) if args.workload == "mold" else (H, BAND)
+    set_level(args.h if args.h is not None else dh, args.band if args.band is not None else db)
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local = int(os.environ.get("LOCAL_RANK", 0))
@@ -194,7 +210,7 @@ def main():
     from implicitcam_b200 import part_gpu
 
     prec = {"fp64": part_gpu.FP64, "mixed": part_gpu.MIXED, "learned": part_gpu.MIXED_LEARNED}[args.precision]
-    b, lo, nb = workload(seed=rank)
+    b, lo, nb = workload(seed=rank, kind=args.workload)
     need = BAND + 8 * H * np.sqrt(3.0)
     g = part_gpu.PartGpu(b, need=need, device=local)
     stream = torch.cuda.ExternalStream(g.stream(), device=local)
@@ -285,7 +301,7 @@ def main():
         achieved = flops / (node_ms * 1e-3)
         cpu = None
         if not args.no_cpu and world == 1:
-            v, cores, sample = cpu_bake_sample(0)
+            v, cores, sample = cpu_bake_sample(0, kind=args.workload)
             cpu = {"value": v, "unit": "voxels/s", "cores": cores, "kind": "port", "sample": sample}
         clocks = read_clocks(clk_path, local)
         out = {
@@ -293,7 +309,8 @@ def main():
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == part_gpu.FP64 else "f32+f64",
             "data": "synthetic",
-            "config": {"workload": f"freeform-top level bake, h={H} mm, band +-{BAND} mm", "part": "freeform_top",
+            "config": {"workload": workload_name(args.workload),
+                       "part": "mold" if args.workload == "mold" else "freeform_top",
                        "seed": "rank", "h_mm": H, "band_mm": BAND, "nb": nb.tolist(), "precision": args.precision,
                        "l2": "flushed (256 MB write) before every step"},
             "speedup_vs_fp64": None if fp64 is None else value / fp64["value"],

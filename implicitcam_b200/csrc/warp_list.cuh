@@ -314,16 +314,21 @@ __device__ __forceinline__ void warp_point(const DPack& P, const WarpCands& W, d
       double d32 = sqrt(double(dotf(rf, rf)));
       // a float distance past the answer by more than its error cannot win
       if (d32 > best + 1e-4 * (1.0 + best)) continue;
-      // The float answer stands where it is well conditioned: converged, away from the
-      // surface (so its sign is sure; about 2e-6 mm of error on the rebased net, within
-      // the mixed form's 1e-7 of the diagonal) and on a sub-patch wholly inside its
-      // face's loops. Everything else (the sign near zero, the loops' parity near their
-      // edges, a stalled float solve) goes to the double polish below.
-      if (fconv && d32 > 1e-3 && s.klass == 1) {
+      // The float answer stands where it is well conditioned: converged and away from
+      // the surface (so its sign is sure; about 2e-6 mm of error on the rebased net,
+      // within the mixed form's 1e-7 of the diagonal). On a sub-patch across its face's
+      // loops the foot's side of the loops is the double parity test at the float foot:
+      // a foot within the float error of a loop moves the answer by the square of that
+      // error. Everything else (the sign near zero, a stalled float solve) goes to the
+      // double polish below.
+      if (fconv && d32 > 1e-3) {
         if (!is_critical_f(p32, ef)) continue;
         float3 nf = f3(ef.ps.y * ef.pt.z - ef.ps.z * ef.pt.y, ef.ps.z * ef.pt.x - ef.ps.x * ef.pt.z,
                        ef.ps.x * ef.pt.y - ef.ps.y * ef.pt.x);
         if (!(dotf(nf, nf) > 0.f) || !(d32 < best)) continue;
+        if (s.klass != 1 &&
+            !trim_inside(P, P.faces[s.face], s.u0 + double(sf) * (s.u1 - s.u0), s.v0 + double(tf) * (s.v1 - s.v0)))
+          continue;
         best = d32;
         sdv = d32 * sgn(-double(dotf(rf, nf)) * P.faces[s.face].sense);
         continue;

@@ -13,7 +13,10 @@
   surface kinds the parts above lack (the sphere and torus have no edges at all);
 - ``boss`` (cylinder, torus fillet, plane cap), ``countersunk_block`` (a hole with a
   cone countersink) and ``dome`` (a cylinder under a hemisphere): the analytic families
-  of a batch of uneven parts.
+  of a batch of uneven parts;
+- ``mold``: a 250 x 200 x 80 mm block with a pocket whose floor is 500 one-span bicubic
+  rational B-spline faces joined along shared B-spline edges, and 40 filleted bosses on
+  its rim.
 
 Random numbers come from the reference checkers' xorshift64 generator
 (crates/icam-check/src/exact_check.rs:45-52) seeded through splitmix64, so that
@@ -339,22 +342,21 @@ def ring(major=4.0, minor=1.5):
     return b
 
 
-def boss(r=3.0, height=5.0, fillet=1.0):
-    """A boss: the can with its top edge rounded by a quarter-torus fillet (bottom plane,
-    cylinder to height - fillet, torus of major r - fillet and minor fillet, top plane
-    of radius r - fillet; three circles, two seams)."""
-    b = SolidBuilder(tol=1e-9)
+def _boss_body(b: SolidBuilder, cx, cy, z0, r, height, fillet):
+    """A boss's cylinder from z0 to z0 + height - fillet, its quarter-torus fillet and its
+    cap plane (radius r - fillet at z0 + height); returns its base circle at z0, whose
+    face below (a disc, or a plane with the circle as a hole) is the caller's."""
     z, x = [0, 0, 1], [1, 0, 0]
     zm = height - fillet
-    f0, fm, f1 = Frame([0, 0, 0], z, x), Frame([0, 0, zm], z, x), Frame([0, 0, height], z, x)
-    va, vm, vt = b.vertex([r, 0, 0]), b.vertex([r, 0, zm]), b.vertex([r - fillet, 0, height])
+    f0, fm, f1 = Frame([cx, cy, z0], z, x), Frame([cx, cy, z0 + zm], z, x), Frame([cx, cy, z0 + height], z, x)
+    va, vm = b.vertex([cx + r, cy, z0]), b.vertex([cx + r, cy, z0 + zm])
+    vt = b.vertex([cx + r - fillet, cy, z0 + height])
     c0 = b.arc(f0, r, 0.0, TAU, va, va)
     cm = b.arc(fm, r, 0.0, TAU, vm, vm)
     ct = b.arc(f1, r - fillet, 0.0, TAU, vt, vt)
     seam_c = b.line(va, vm)
-    # the fillet's seam: a quarter circle in the xz plane from (r, 0, zm) up to (r - f, 0, h)
-    seam_t = b.arc(Frame([r - fillet, 0, zm], [0, -1, 0], [1, 0, 0]), fillet, 0.0, math.pi / 2, vm, vt)
-    _plane_face(b, f0, -1, [[(c0, True)]])
+    # the fillet's seam: a quarter circle in the xz plane from (r, zm) up to (r - f, height)
+    seam_t = b.arc(Frame([cx + r - fillet, cy, z0 + zm], [0, -1, 0], [1, 0, 0]), fillet, 0.0, math.pi / 2, vm, vt)
     _plane_face(b, f1, +1, [[(ct, False)]])
     lo, hi = _pad([0.0, 0.0], [TAU, zm])
     cyl = b.face(CYLINDER, +1, f0, a=r, lo=[0.0, lo[1]], hi=[TAU, hi[1]], period=[TAU, 0.0])
@@ -372,6 +374,16 @@ def boss(r=3.0, height=5.0, fillet=1.0):
         (ct, True, line_pcurve([TAU, math.pi / 2], [0.0, math.pi / 2])),
         (seam_t, True, None),
     ])
+    return c0
+
+
+def boss(r=3.0, height=5.0, fillet=1.0):
+    """A boss: the can with its top edge rounded by a quarter-torus fillet (bottom plane,
+    cylinder to height - fillet, torus of major r - fillet and minor fillet, top plane
+    of radius r - fillet; three circles, two seams)."""
+    b = SolidBuilder(tol=1e-9)
+    c0 = _boss_body(b, 0.0, 0.0, 0.0, r, height, fillet)
+    _plane_face(b, Frame([0, 0, 0], [0, 0, 1], [1, 0, 0]), -1, [[(c0, True)]])
     return b
 
 
@@ -457,6 +469,128 @@ def countersunk_block(size=(40.0, 30.0, 20.0), center=(20.0, 15.0), r=4.0, sink=
         (cm, True, line_pcurve([TAU, 0.0], [0.0, 0.0])),
         (seam_k, False, None),
     ])
+    return b
+
+
+def mold(seed=0, size=(250.0, 200.0, 80.0), rim=25.0, fu=25, fv=20, floor=40.0, bumps=10, bosses=40):
+    """A mold cavity: a size block with a pocket `rim` mm in from its sides, the pocket's
+    floor a clamped bicubic rational B-spline of fu x fv spans (heights floor plus
+    `bumps` seeded Gaussians, amplitude U[2,8] mm, sigma U[10,40] mm; weights U[0.8,1.2])
+    cut at its knots into fu x fv faces of one span each, so neighbouring faces join C2
+    along shared B-spline edges; four vertical pocket walls; and `bosses` filleted bosses
+    (cylinder, quarter-torus fillet, cap; radius U[3,6] mm, height U[5,15] mm) standing
+    on the rim. About 640 faces."""
+    X, Y, Z = size
+    ax, ay, bx, by = rim, rim, X - rim, Y - rim
+    rng = Rng(seed)
+    g = []
+    for _ in range(bumps):
+        g.append((rng.uniform(2.0, 8.0), rng.uniform(10.0, 40.0), rng.uniform(ax, bx), rng.uniform(ay, by)))
+    nu, nv = fu + 3, fv + 3
+    net = np.zeros((nu, nv, 4))
+    for i in range(nu):
+        for j in range(nv):
+            x = ax + (bx - ax) * i / (nu - 1)
+            y = ay + (by - ay) * j / (nv - 1)
+            zz = floor + sum(a * math.exp(-((x - cx) ** 2 + (y - cy) ** 2) / (2 * s * s)) for a, s, cx, cy in g)
+            w = rng.uniform(0.8, 1.2)
+            net[i, j] = [x * w, y * w, zz * w, w]
+    ku = [0.0] * 4 + [k / fu for k in range(1, fu)] + [1.0] * 4
+    kv = [0.0] * 4 + [k / fv for k in range(1, fv)] + [1.0] * 4
+    patches, ub, vb = surface_spans(3, 3, ku, kv, net)
+    b = SolidBuilder(tol=1e-9)
+    pt = lambda hh: hh[:3] / hh[3]  # noqa: E731
+    # the floor's vertices at its knot grid, and its iso-curve edges (increasing parameter)
+    fvx = {}
+    for a in range(fu + 1):
+        for c in range(fv + 1):
+            pa, pc = min(a, fu - 1), min(c, fv - 1)
+            fvx[a, c] = b.vertex(pt(patches[pa, pc, -1 if a == fu else 0, -1 if c == fv else 0]))
+    eu = {}  # u = ub[a], from vb[c] to vb[c + 1]
+    for a in range(fu + 1):
+        for c in range(fv):
+            piece = patches[a, c, 0, :, :] if a < fu else patches[fu - 1, c, -1, :, :]
+            eu[a, c] = b.spline([piece.copy()], fvx[a, c], fvx[a, c + 1])
+    ev = {}  # v = vb[c], from ub[a] to ub[a + 1]
+    for a in range(fu):
+        for c in range(fv + 1):
+            piece = patches[a, c, :, 0, :] if c < fv else patches[a, fv - 1, :, -1, :]
+            ev[a, c] = b.spline([piece.copy()], fvx[a, c], fvx[a + 1, c])
+    for a in range(fu):
+        for c in range(fv):
+            u0, u1, v0, v1 = ub[a], ub[a + 1], vb[c], vb[c + 1]
+            f = b.face(NURBS, +1, lo=[u0, v0], hi=[u1, v1],
+                       nurbs=(patches[a:a + 1, c:c + 1].copy(), ub[a:a + 2].copy(), vb[c:c + 2].copy()))
+            b.loop(f, [
+                (ev[a, c], False, line_pcurve([u0, v0], [u1, v0])),
+                (eu[a + 1, c], False, line_pcurve([u1, v0], [u1, v1])),
+                (ev[a, c + 1], True, line_pcurve([u1, v1], [u0, v1])),
+                (eu[a, c], True, line_pcurve([u0, v1], [u0, v0])),
+            ])
+    # the block's corners, the rim's corners at the top and the pocket walls' vertical edges
+    cb = {}
+    for i, xx in enumerate((0.0, X)):
+        for j, yy in enumerate((0.0, Y)):
+            for k, zz in enumerate((0.0, Z)):
+                cb[i, j, k] = b.vertex([xx, yy, zz])
+    L = lambda p, q: b.line(cb[p], cb[q])  # noqa: E731
+    eb = [L((0, 0, 0), (1, 0, 0)), L((1, 0, 0), (1, 1, 0)), L((1, 1, 0), (0, 1, 0)), L((0, 1, 0), (0, 0, 0))]
+    et = [L((0, 0, 1), (1, 0, 1)), L((1, 0, 1), (1, 1, 1)), L((1, 1, 1), (0, 1, 1)), L((0, 1, 1), (0, 0, 1))]
+    es = {ij: L((*ij, 0), (*ij, 1)) for ij in ((0, 0), (1, 0), (1, 1), (0, 1))}
+    rv = {(0, 0): b.vertex([ax, ay, Z]), (1, 0): b.vertex([bx, ay, Z]), (1, 1): b.vertex([bx, by, Z]),
+          (0, 1): b.vertex([ax, by, Z])}
+    fc = {(0, 0): fvx[0, 0], (1, 0): fvx[fu, 0], (1, 1): fvx[fu, fv], (0, 1): fvx[0, fv]}
+    rl = [b.line(rv[0, 0], rv[1, 0]), b.line(rv[1, 0], rv[1, 1]), b.line(rv[1, 1], rv[0, 1]), b.line(rv[0, 1], rv[0, 0])]
+    wv = {ij: b.line(fc[ij], rv[ij]) for ij in fc}  # up from the floor's corners
+    # outer block: bottom and four sides
+    _plane_face(b, Frame([0, 0, 0], [0, 0, 1], [1, 0, 0]), -1,
+                [[(eb[3], True), (eb[2], True), (eb[1], True), (eb[0], True)]])
+    _plane_face(b, Frame([0, 0, 0], [0, -1, 0], [1, 0, 0]), +1,
+                [[(eb[0], False), (es[1, 0], False), (et[0], True), (es[0, 0], True)]])
+    _plane_face(b, Frame([X, 0, 0], [1, 0, 0], [0, 1, 0]), +1,
+                [[(eb[1], False), (es[1, 1], False), (et[1], True), (es[1, 0], True)]])
+    _plane_face(b, Frame([X, Y, 0], [0, 1, 0], [-1, 0, 0]), +1,
+                [[(eb[2], False), (es[0, 1], False), (et[2], True), (es[1, 1], True)]])
+    _plane_face(b, Frame([0, Y, 0], [-1, 0, 0], [0, -1, 0]), +1,
+                [[(eb[3], False), (es[0, 0], False), (et[3], True), (es[0, 1], True)]])
+    # the pocket's walls, outward into the pocket: each runs along the floor's boundary
+    # edges, up a corner, back along the rim, down the other corner (counterclockwise seen
+    # from the pocket)
+    front = [(ev[a, 0], True) for a in reversed(range(fu))]  # y = ay, x from bx to ax
+    _plane_face(b, Frame([bx, ay, 0], [0, 1, 0], [-1, 0, 0]), +1,
+                [front + [(wv[0, 0], False), (rl[0], False), (wv[1, 0], True)]])
+    right = [(eu[fu, c], True) for c in reversed(range(fv))]  # x = bx, y from by to ay
+    _plane_face(b, Frame([bx, by, 0], [-1, 0, 0], [0, -1, 0]), +1,
+                [right + [(wv[1, 0], False), (rl[1], False), (wv[1, 1], True)]])
+    back = [(ev[a, fv], False) for a in range(fu)]  # y = by, x from ax to bx
+    _plane_face(b, Frame([ax, by, 0], [0, -1, 0], [1, 0, 0]), +1,
+                [back + [(wv[1, 1], False), (rl[2], False), (wv[0, 1], True)]])
+    left = [(eu[0, c], False) for c in range(fv)]  # x = ax, y from ay to by
+    _plane_face(b, Frame([ax, ay, 0], [1, 0, 0], [0, 1, 0]), +1,
+                [left + [(wv[0, 1], False), (rl[3], False), (wv[0, 0], True)]])
+    # bosses on the rim's centre line, evenly spaced by arc length
+    half = rim / 2
+    px, py = X - rim, Y - rim  # the centre line's rectangle sides
+    per = 2 * (px + py)
+    holes = []
+    for k in range(bosses):
+        t = (k + 0.5) * per / bosses
+        if t < px:
+            cx, cy = half + t, half
+        elif t < px + py:
+            cx, cy = X - half, half + (t - px)
+        elif t < 2 * px + py:
+            cx, cy = X - half - (t - px - py), Y - half
+        else:
+            cx, cy = half, Y - half - (t - 2 * px - py)
+        r = rng.uniform(3.0, 6.0)
+        hgt = rng.uniform(5.0, 15.0)
+        fil = min(0.3 * r, 0.4 * hgt) * rng.uniform(0.5, 1.0)
+        holes.append([(_boss_body(b, cx, cy, Z, r, hgt, fil), True)])
+    # the top: the block's outline, the pocket's rim as a hole, the bosses' bases as holes
+    _plane_face(b, Frame([0, 0, Z], [0, 0, 1], [1, 0, 0]), +1,
+                [[(et[0], False), (et[1], False), (et[2], False), (et[3], False)],
+                 [(rl[3], True), (rl[2], True), (rl[1], True), (rl[0], True)]] + holes)
     return b
 
 
