@@ -316,7 +316,9 @@ def main():
             "speedup_vs_fp64": None if fp64 is None else value / fp64["value"],
             "fp64": fp64, "error_vs_fp64": error, "seednet": seednet,
             "bricks_read": st["bricks_read"], "bricks_stored": st["bricks_words"],
+            "bricks_settled": st["bricks_settled"],
             "nodes_exact": st["nodes_exact"], "nodes_undecided": st["nodes_undecided"],
+            "nodes_exact_per_s": st["nodes_exact"] * args.steps / (total_ms * 1e-3),
             "stage_ms": {"decide": st["ms_decide"], "nodes": st["ms_nodes"], "assemble": st["ms_post"]},
             "gpu_launches": int(st["kernel_launches"]) * args.steps,
             "e2e": {"value": e2e_value, "unit": "voxels/s", "h2d_bytes_per_step": 512,

@@ -434,6 +434,7 @@ static int bake_level(IcamPack* pk, double h, const double lo[3], const int64_t 
     b.leaves = pk->leaves;
     b.n_leaves = int32_t(pk->leaves_host.size());
     b.mixed = precision != ICAM_FP64;
+    b.kind_only = 1;
     if ((r = learned_starts(pk, precision, &b))) return r;
     b.words_out = (uint32_t*)d_words;
     b.kind_out = (int32_t*)d_kind;
@@ -478,6 +479,7 @@ static int bake_level(IcamPack* pk, double h, const double lo[3], const int64_t 
     stats->nodes_undecided = R ? int64_t(st[2]) : 0;
     stats->pairs = R ? int64_t(st[4]) : 0;
     for (int k = 0; k < 5; k++) stats->census[k] = R ? int64_t(st[6 + k]) : 0;
+    stats->bricks_settled = R ? int64_t(st[11]) : 0;
     stats->kernel_launches = launches;
     float ms;
     cudaEventElapsedTime(&ms, ev[0], ev[1]);

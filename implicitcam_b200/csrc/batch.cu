@@ -395,6 +395,7 @@ int icam_batch_bake(IcamBatch* bt, const IcamBatchLevel* levels, int precision, 
   a.dcs = static_cast<const double*>(dcs);
   a.n = R;
   a.mixed = precision != ICAM_FP64;
+  a.kind_only = 1;
   a.words_out = static_cast<uint32_t*>(words);
   a.kind_out = static_cast<int32_t*>(kind);
   a.stats = bt->d_stats;
@@ -474,6 +475,7 @@ int icam_batch_bake(IcamBatch* bt, const IcamBatchLevel* levels, int precision, 
     stats->bricks_words = pslot[n];
     stats->nodes_exact = int64_t(st[0]);
     stats->nodes_undecided = int64_t(st[2]);
+    stats->bricks_settled = int64_t(st[11]);
     stats->kernel_launches = launches;
     stats->warps = bt->warps;
     stats->graph_replayed = replayed ? 1 : 0;

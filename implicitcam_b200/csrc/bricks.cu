@@ -174,6 +174,21 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 2) k_bricks_t(BrickArgs a) {
       }
       continue;
     }
+    // ---- 0b. every node on one side of the surface by more than an i16 step, known from
+    // the centre alone (|d(node) - dc| <= half sqrt(3)): the brick's kind is the centre's
+    // sign. The packing (partcache.rs:962-970) makes a brick AIR when every stored value
+    // is > 0 and SOLID when every one is <= 0; a node read exactly stores
+    // round(d / clamp * 32767), at least 1 for d > clamp / 32767 and at most -1 for
+    // d < -clamp / 32767, and a node settled from another stores the clamp with that
+    // node's sign, the same. A level bake keeps no words of such a brick, so none are
+    // written. Same map as reading it.
+    if (a.kind_only && isfinite(dc) && fabs(dc) - half * SQRT3 > clamp * (1.0 / 32767.0) + 1e-9 * (1.0 + fabs(dc))) {
+      if (lane == 0) {
+        if (a.kind_out) a.kind_out[bi] = dc > 0 ? 1 : 2;
+        if (a.stats) atomicAdd(&a.stats[11], 1ull);
+      }
+      continue;
+    }
     // ---- 1. list
     int n = warp_list(P, leaves, n_leaves, c, reach, S.u.list.code, S.u.list.lb, S.u.list.fr, &S.n, lane);
     const bool overflow = n > MAXC;

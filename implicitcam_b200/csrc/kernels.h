@@ -40,14 +40,16 @@ struct BrickArgs {
   const int32_t* leaves;  // the tree's leaf nodes
   int32_t n_leaves;
   int32_t mixed;          // 1: single-precision bulk with double polish
+  int32_t kind_only;      // 1 (a level bake): a brick whose every node lies on one side of
+                          //   the surface by more than an i16 step gets its kind alone
   const float* net_feat;  // the seed network's sub-patch features and weights
   const void* net_w;      //   (seednet.cuh), or null: centre starts
   double* d_out;          // optional n x 729 values
   int8_t* flag_out;       // optional n x 729 flags
   uint32_t* words_out;    // optional n x 365 packed words
   int32_t* kind_out;      // optional n kinds (0 words, 1 air, 2 solid)
-  // exact, far, undecided, bridged, pairs, overflows, census [6..10]; [15] the kernel's
-  // brick counter. Zeroed before each launch; null for none (bricks then taken in a
+  // exact, far, undecided, bridged, pairs, overflows, census [6..10], bricks given their
+  // kind from the centre alone [11]; [15] the kernel's brick counter. Zeroed before each launch; null for none (bricks then taken in a
   // fixed order).
   unsigned long long* stats;
 };

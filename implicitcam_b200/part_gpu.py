@@ -33,7 +33,7 @@ class IcamBakeStats(C.Structure):
         ("nodes_exact", C.c_int64), ("nodes_far", C.c_int64), ("nodes_undecided", C.c_int64),
         ("pairs", C.c_int64), ("fallback_nodes", C.c_int64), ("kernel_launches", C.c_int64),
         ("ms_decide", C.c_double), ("ms_cull", C.c_double), ("ms_nodes", C.c_double), ("ms_post", C.c_double),
-        ("census", C.c_int64 * 5),
+        ("census", C.c_int64 * 5), ("bricks_settled", C.c_int64),
     ]
 
     def as_dict(self):
@@ -55,7 +55,8 @@ class IcamBatchStats(C.Structure):
     _fields_ = [("parts", C.c_int64), ("boxes_read", C.c_int64), ("bricks_read", C.c_int64),
                 ("bricks_words", C.c_int64), ("nodes_exact", C.c_int64), ("nodes_undecided", C.c_int64),
                 ("kernel_launches", C.c_int64), ("warps", C.c_int32), ("graph_replayed", C.c_int32),
-                ("tune_ms", C.c_double * 3), ("ms_decide", C.c_double), ("ms_bricks", C.c_double)]
+                ("tune_ms", C.c_double * 3), ("ms_decide", C.c_double), ("ms_bricks", C.c_double),
+                ("bricks_settled", C.c_int64)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "tune_ms"}

@@ -62,7 +62,7 @@ typedef struct IcamPackOptions {
 
 typedef struct IcamBakeStats {
   int64_t boxes_read;      /* box centres read by the decision */
-  int64_t bricks_read;     /* bricks whose nodes were read */
+  int64_t bricks_read;     /* bricks the decision reads (its boxes of one brick) */
   int64_t bricks_words;    /* of those, bricks stored as words (not air or solid) */
   int64_t nodes_exact;     /* flag 0 nodes */
   int64_t nodes_far;       /* flag 1 nodes, signed by the fill */
@@ -76,6 +76,10 @@ typedef struct IcamBakeStats {
    * faces, B-spline spans (distinct spans of the sub-patches listed), line or arc
    * edges, spline edge pieces, vertices. */
   int64_t census[5];
+  /* Read bricks whose every node lies on one side of the surface by more than an i16
+   * step, known from the brick's centre distance (the field is 1-Lipschitz): air or
+   * solid without reading their nodes. */
+  int64_t bricks_settled;
 } IcamBakeStats;
 
 /* Packs the solid for the device (PartGpu::new, partgpu.rs:132; Exact::gpu_pack,
@@ -200,6 +204,7 @@ typedef struct IcamBatchStats {
   int32_t graph_replayed;  /* 1: the post-decision graph was replayed, 0: captured */
   double tune_ms[3];       /* the tuning's times for 1, 2 and 4 warps a block */
   double ms_decide, ms_bricks;
+  int64_t bricks_settled;  /* as IcamBakeStats::bricks_settled */
 } IcamBatchStats;
 
 /* A batch over n packs on one device (a pack may appear more than once, e.g. to bake one
