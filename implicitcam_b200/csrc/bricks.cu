@@ -182,7 +182,7 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 2) k_bricks_t(BrickArgs a) {
     // d < -clamp / 32767, and a node settled from another stores the clamp with that
     // node's sign, the same. A level bake keeps no words of such a brick, so none are
     // written. Same map as reading it.
-    if (a.kind_only && isfinite(dc) && fabs(dc) - half * SQRT3 > clamp * (1.0 / 32767.0) + 1e-9 * (1.0 + fabs(dc))) {
+    if (a.kind_only && isfinite(dc) && settles_by_sign(dc, h, clamp)) {
       if (lane == 0) {
         if (a.kind_out) a.kind_out[bi] = dc > 0 ? 1 : 2;
         if (a.stats) atomicAdd(&a.stats[11], 1ull);

@@ -70,6 +70,13 @@ __device__ void decide_box(const DecideArgs& a, long long size, const Box4& b, d
     const long long half = size / 2;
     Box4 kids[8];
     int nk = 0;
+    // Bricks (children of size 1) settled by this box's exact centre distance sd: a child
+    // whose centre lies within sd's empty ball has |v| <= |sd| + reach < r + clamp, so its
+    // own reading would find it neither air nor material and read it; and when
+    // |sd| - reach (a bound on |v| with sd's sign) already settles the brick by sign, the
+    // brick kernel needs nothing more of it. Such a child is read with that bound as its
+    // centre distance instead of being queried.
+    const bool by_bound = half == 1 && isfinite(sd) && sd != 0.0;
     for (int q = 0; q < 8; q++) {
       Box4 k;
       k.x = b.x + half * (q & 1);
@@ -81,6 +88,22 @@ __device__ void decide_box(const DecideArgs& a, long long size, const Box4& b, d
                        a.lo[2] + side * (k.z + half) + a.clamp);
       k.reach = len((klo + khi) * 0.5 - c);
       k.parent_sd = sd;
+      if (by_bound) {
+        const double rk = 0.5 * len(khi - klo);
+        const double bound = fabs(sd) - k.reach;
+        const double dcb = copysign(bound, sd);
+        if (fabs(sd) + k.reach < (rk + a.clamp) * (1.0 - 1e-12) && bound > 0.0 &&
+            settles_by_sign(dcb, a.h, a.clamp, 1e-9 * (1.0 + a.clamp))) {
+          const long long idx = k.x + nb0 * (k.y + nb1 * k.z);
+          a.map[idx] = 0xfffffff0u;  // read
+          unsigned long long slot = atomicAdd(a.n_read, 1ull);
+          if (slot < (unsigned long long)a.read_cap) {
+            a.read_idx[slot] = idx;
+            a.read_dc[slot] = dcb;
+          }
+          continue;
+        }
+      }
       kids[nk++] = k;
     }
     // together, so that the next level's warps take neighbouring boxes

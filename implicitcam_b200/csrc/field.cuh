@@ -9,6 +9,15 @@ namespace icam {
 
 constexpr double SQRT3 = 1.7320508075688772;
 
+// A read brick (cell side h) whose centre distance dc puts every node on one side of the
+// surface by more than an i16 step of the clamp (the field is 1-Lipschitz and a node is
+// at most 4h sqrt(3) from the centre): the brick packs to AIR (dc > 0) or SOLID whatever
+// its nodes read, every exactly read value quantising to at least one step of dc's sign.
+// `extra` widens the test (the decision leaves room for the brick kernel's own rounding).
+__host__ __device__ inline bool settles_by_sign(double dc, double h, double clamp, double extra = 0.0) {
+  return fabs(dc) - 4.0 * h * SQRT3 > clamp * (1.0 / 32767.0) + 1e-9 * (1.0 + fabs(dc)) + extra;
+}
+
 // What a point's evaluation keeps: the least distance found, its signed value, and
 // the least lower bound among features it could not decide.
 struct Acc {
