@@ -270,17 +270,20 @@ int icam_bricks(IcamPack* pk, const double* first_nodes, size_t n, double h, dou
 // read bricks sorted in brick order (partcache.rs:486); results in scratch 3, 9, 10.
 // The first boxes of a level's decision, on the grid aligned on the origin
 // (partcache.rs:250-270); returns their size in bricks.
-long long first_boxes(const LevelDesc& L, std::vector<Box4>* out) {
+long long first_boxes(const LevelDesc& L, std::vector<Box4>* out, long long dims[3]) {
   const int64_t* nb = L.nb;
   const double* lo = L.lo;
   const double* origin = L.has_origin ? L.origin : nullptr;
   long long nbmax = std::max(nb[0], std::max(nb[1], nb[2]));
   long long size = 1;
   // The reference starts from one box over the whole level; here from boxes of at most
-  // 32 bricks a side (measured on the freeform part at h = 0.1: decide 56 -> 44 ms). Every box a coarser start would settle is settled the same way by
+  // 8 bricks a side. Every box a coarser start would settle is settled the same way by
   // the boxes inside it (grown by the clamp, a child's ball lies in its parent's), so the
-  // map is the same, and the few coarse boxes, each read within tens of mm, are spared.
-  while (size < nbmax && size < 32) size *= 2;
+  // map is the same, and the coarse boxes, each read within tens of mm, are spared; the
+  // first boxes far from the part take their sign from a neighbour (k_first_signs)
+  // instead of a reading without a bound. Measured on the freeform part at h = 0.1:
+  // one box 56 ms, boxes of 32 bricks 44 ms, boxes of 8 bricks 28 ms.
+  while (size < nbmax && size < 8) size *= 2;
   double side = 8.0 * L.h;
   double o[3] = {origin ? origin[0] - L.h : lo[0] - 0.0, origin ? origin[1] - L.h : lo[1], origin ? origin[2] - L.h : lo[2]};
   long long g0[3], start[3];
@@ -293,6 +296,8 @@ long long first_boxes(const LevelDesc& L, std::vector<Box4>* out) {
   for (long long z = start[2]; z < nb[2]; z += size)
     for (long long y = start[1]; y < nb[1]; y += size)
       for (long long x = start[0]; x < nb[0]; x += size) out->push_back({x, y, z, NAN, INFINITY});
+  if (dims)
+    for (int k = 0; k < 3; k++) dims[k] = (nb[k] - start[k] + size - 1) / size;
   return size;
 }
 
@@ -317,7 +322,10 @@ int decide_level(IcamPack* pk, const LevelDesc& L, DecideOut* out) {
     return r;
   CK(cudaMemsetAsync(d_cnt, 0, 4 * sizeof(unsigned long long), s));
   std::vector<Box4> first;
-  long long size = first_boxes(L, &first);
+  long long dims[3];
+  long long size = first_boxes(L, &first, dims);
+  void* d_first;
+  if ((r = scratch(pk, 16, first.size() * (sizeof(double) + 1) + 16, &d_first))) return r;
   CK(cudaMemcpyAsync(d_cur, first.data(), first.size() * sizeof(Box4), cudaMemcpyHostToDevice, s));
   int64_t ncur = int64_t(first.size()), boxes_read = 0;
   unsigned long long* cnt = (unsigned long long*)d_cnt;
@@ -340,9 +348,15 @@ int decide_level(IcamPack* pk, const LevelDesc& L, DecideOut* out) {
     a.read_dc = (double*)d_rdc;
     a.read_cap = total;
     a.n_read = cnt + 1;
+    const bool is_first = launches == 0;
+    if (is_first) {
+      a.first_sd = static_cast<double*>(d_first);
+      a.first_sign = reinterpret_cast<int8_t*>(static_cast<double*>(d_first) + ncur);
+      for (int k = 0; k < 3; k++) a.first_dims[k] = dims[k];
+    }
     CK(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), s));
-    launch_decide(a, s);
-    launches++;
+    launch_decide(a, s, is_first);
+    launches += is_first ? 2 : 1;
     CK(cudaGetLastError());
     unsigned long long nn = 0;
     CK(cudaMemcpyAsync(&nn, cnt, sizeof(nn), cudaMemcpyDeviceToHost, s));

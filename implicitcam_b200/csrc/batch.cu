@@ -95,7 +95,7 @@ struct IcamBatch {
     void* p = nullptr;
     size_t n = 0;
   };
-  Buf buf[24];
+  Buf buf[25];
   PartParams* d_parts = nullptr;
   unsigned long long* d_stats = nullptr;
   int warps = 0;  // the tuned tiling (0: not tuned yet)
@@ -247,7 +247,7 @@ int icam_batch_bake(IcamBatch* bt, const IcamBatchLevel* levels, int precision, 
     L.h = lv.h, L.clamp = lv.clamp;
     for (int k = 0; k < 3; k++) L.lo[k] = lv.lo[k], L.nb[k] = lv.nb[k], L.origin[k] = lv.origin[k];
     L.has_origin = lv.has_origin != 0;
-    const long long size = first_boxes(L, &first[i]);
+    const long long size = first_boxes(L, &first[i], args[2 * i].first_dims);
     int lg = 0;
     while ((1LL << lg) < size) lg++;
     rounds = std::max(rounds, lg + 1);
@@ -265,9 +265,15 @@ int icam_batch_bake(IcamBatch* bt, const IcamBatchLevel* levels, int precision, 
     a.next_cap = box_off[i + 1] - box_off[i];
     a.read_cap = total;
   }
-  void *boxes[2], *maps_all, *ridx, *rdc, *cnt, *groups, *d_args, *d_roff, *keys[2];
+  void *boxes[2], *maps_all, *ridx, *rdc, *cnt, *groups, *d_args, *d_roff, *keys[2], *firsts_sd;
   const int64_t BX = box_off[n], LV = lvl_off[n];
+  std::vector<int64_t> first_off(n + 1, 0);  // the first boxes' values, then their signs
+  for (int i = 0; i < n; i++) first_off[i + 1] = first_off[i] + int64_t(first[i].size());
   int r;
+  if ((r = bbuf(bt, 24, first_off[n] * (sizeof(double) + 1) + 16, &firsts_sd))) {
+    cleanup();
+    return r;
+  }
   if ((r = bbuf(bt, 12, BX * sizeof(Box4), &boxes[0])) || (r = bbuf(bt, 13, BX * sizeof(Box4), &boxes[1])) ||
       (r = bbuf(bt, 14, LV * sizeof(uint32_t), &maps_all)) || (r = bbuf(bt, 15, LV * sizeof(int64_t), &ridx)) ||
       (r = bbuf(bt, 16, LV * sizeof(double), &rdc)) ||
@@ -295,6 +301,8 @@ int icam_batch_bake(IcamBatch* bt, const IcamBatchLevel* levels, int precision, 
     b.boxes = static_cast<Box4*>(boxes[1]) + box_off[i];
     b.next = static_cast<Box4*>(boxes[0]) + box_off[i];
     b.n_next = c + 2 * i;
+    a.first_sd = static_cast<double*>(firsts_sd) + first_off[i];
+    a.first_sign = reinterpret_cast<int8_t*>(static_cast<double*>(firsts_sd) + first_off[n]) + first_off[i];
     c0[2 * i] = first[i].size();
     if (!first[i].empty())
       BCK(cudaMemcpyAsync(static_cast<Box4*>(boxes[0]) + box_off[i], first[i].data(), first[i].size() * sizeof(Box4),
@@ -312,7 +320,7 @@ int icam_batch_bake(IcamBatch* bt, const IcamBatchLevel* levels, int precision, 
   db.err = reinterpret_cast<int*>(c + 3 * n + 1);
   launch_decide_batch(db, rounds, s);
   BCK(cudaGetLastError());
-  int64_t launches = 2 * rounds;
+  int64_t launches = 2 * rounds + 1;
   BCK(cudaMemcpyAsync(c0.data(), c, c0.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
   BCK(cudaStreamSynchronize(s));
   if (c0[3 * n + 1] != 0) {

@@ -7,6 +7,9 @@
 namespace icam {
 
 constexpr int DWARPS = 4;  // box groups a block works on at once, one a warp
+// first_sign of a first box: +1 / -1 its exact value's sign, 0 none (not exact, or on the
+// surface), pending (past its cut, sign not known), then air or material once known
+constexpr int8_t FS_PENDING = 2, FS_AIR = 3, FS_SOLID = -3;
 
 struct DecideSmem {
   uint32_t tcode[MAXC];  // the list before its ranking, and the walk's frontier
@@ -118,7 +121,7 @@ __device__ void decide_box(const DecideArgs& a, long long size, const Box4& b, d
 // sub-patches seeded there), every centre's value capped at the cut by the shared walk,
 // then each box decided.
 __device__ __forceinline__ void decide_group(const DecideArgs& a, const Box4* boxes, int64_t n, long long size,
-                                             int64_t g0, DecideSmem& S, int lane) {
+                                             int64_t g0, DecideSmem& S, int lane, bool first) {
   const DPack& P = a.P;
   const double side = 8.0 * a.h;
   const int64_t i = g0 + lane;
@@ -166,15 +169,97 @@ __device__ __forceinline__ void decide_group(const DecideArgs& a, const Box4* bo
   double v;
   int f;
   warp_point<false>(P, W, c, gc, live, cut, lane, &v, &f);
-  if (live) decide_box(a, size, b, c, r, cut, v, f);
+  if (live) {
+    if (first) {
+      // a first box past its cut (air or material, its sign not known: it has no parent)
+      // waits for k_first_signs; an exact value is a sign its neighbours may take
+      a.first_sd[i] = f == 0 ? v : NAN;
+      a.first_sign[i] = f == 1 ? FS_PENDING : ((f == 0 && v != 0.0) ? (v > 0 ? 1 : -1) : 0);
+    }
+    if (!(first && f == 1)) decide_box(a, size, b, c, r, cut, v, f);
+  }
   __syncwarp();
 }
+
+// The centre, radius and cut of a box of `size` bricks (as decide_group computes them).
+__device__ __forceinline__ void box_geometry(const DecideArgs& a, const Box4& b, long long size, double3* c, double* r,
+                                             double* cut) {
+  const double side = 8.0 * a.h;
+  double3 lo = mk(a.lo[0] + side * b.x - a.clamp, a.lo[1] + side * b.y - a.clamp, a.lo[2] + side * b.z - a.clamp);
+  double3 hi = mk(a.lo[0] + side * (b.x + size) + a.clamp, a.lo[1] + side * (b.y + size) + a.clamp,
+                  a.lo[2] + side * (b.z + size) + a.clamp);
+  *c = (lo + hi) * 0.5;
+  *r = 0.5 * len(hi - lo);
+  *cut = (*r + a.clamp) * (1.0 + 1e-4);
+}
+
+// The first boxes past their cut (no feature within it, so air or material; with no
+// parent, their sign is not known), one block a level. A box's sign is that of any box
+// whose centre lies within its cut and whose sign is known: the cut's ball holds no
+// surface. Known signs spread from the boxes read exactly through the grid's face
+// neighbours until none changes (at most n sweeps); a box then known fills its map
+// entries; one no neighbour reached (no box of the level read exactly within its chain)
+// is read without a bound and decided as any other.
+__device__ void first_signs(const DecideArgs& a, int64_t n) {
+  const long long fx = a.first_dims[0], fy = a.first_dims[1], fz = a.first_dims[2];
+  volatile int8_t* sg = a.first_sign;
+  __shared__ int changed;
+  for (int64_t sweep = 0; sweep <= n; sweep++) {
+    __syncthreads();
+    if (threadIdx.x == 0) changed = 0;
+    __syncthreads();
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+      if (sg[i] != FS_PENDING) continue;
+      const long long ix = i % fx, iy = (i / fx) % fy, iz = i / (fx * fy);
+      double3 ci, cj;
+      double ri, cuti, rj, cutj;
+      box_geometry(a, a.boxes[i], a.size, &ci, &ri, &cuti);
+      int8_t got = 0;
+      for (int d = 0; d < 6 && !got; d++) {
+        const long long jx = ix + (d == 0) - (d == 1), jy = iy + (d == 2) - (d == 3), jz = iz + (d == 4) - (d == 5);
+        if (jx < 0 || jy < 0 || jz < 0 || jx >= fx || jy >= fy || jz >= fz) continue;
+        const int64_t j = jx + fx * (jy + fy * jz);
+        const int8_t sj = sg[j];
+        if (sj == 0 || sj == FS_PENDING) continue;
+        box_geometry(a, a.boxes[j], a.size, &cj, &rj, &cutj);
+        if (len(cj - ci) < cuti * (1.0 - 1e-6)) got = sj > 0 ? FS_AIR : FS_SOLID;
+      }
+      if (got) {
+        sg[i] = got;
+        changed = 1;
+      }
+    }
+    __syncthreads();
+    if (!changed) break;
+  }
+  __syncthreads();
+  const long long nb0 = a.nb[0], nb1 = a.nb[1], nb2 = a.nb[2];
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+    const int8_t si = sg[i];
+    const Box4 b = a.boxes[i];
+    if (si == FS_AIR || si == FS_SOLID) {
+      const uint32_t val = si == FS_AIR ? 0xffffffffu : 0xfffffffeu;
+      for (long long z = max(b.z, 0LL); z < min(b.z + a.size, nb2); z++)
+        for (long long y = max(b.y, 0LL); y < min(b.y + a.size, nb1); y++)
+          for (long long x = max(b.x, 0LL); x < min(b.x + a.size, nb0); x++) a.map[x + nb0 * (y + nb1 * z)] = val;
+    } else if (si == FS_PENDING) {
+      double3 c;
+      double r, cut, v;
+      int f;
+      box_geometry(a, b, a.size, &c, &r, &cut);
+      point_fallback(a.P, c, INFINITY, &v, &f);
+      decide_box(a, a.size, b, c, r, cut, v, f);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) k_first_signs(DecideArgs a, int64_t n) { first_signs(a, n); }
 
 __global__ void __launch_bounds__(DWARPS * 32, 2) k_decide_w(DecideArgs a) {
   __shared__ DecideSmem smem[DWARPS];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int64_t g0 = (int64_t(blockIdx.x) * DWARPS + warp) * 32; g0 < a.n; g0 += int64_t(gridDim.x) * DWARPS * 32)
-    decide_group(a, a.boxes, a.n, a.size, g0, smem[warp], lane);
+    decide_group(a, a.boxes, a.n, a.size, g0, smem[warp], lane, a.first_sd != nullptr);
 }
 
 // A batch's round (one box size a part): the counts the last round appended become this
@@ -214,16 +299,23 @@ __global__ void __launch_bounds__(DWARPS * 32, 2) k_decide_batch(DecideBatchArgs
     }
     const DecideArgs& a = b.args[2 * lo + (round & 1)];
     const int64_t n = int64_t(b.cnt[2 * lo + (round & 1)]);
-    decide_group(a, a.boxes, n, a.size >> round, (g - b.groups[lo]) * 32, smem[warp], lane);
+    decide_group(a, a.boxes, n, a.size >> round, (g - b.groups[lo]) * 32, smem[warp], lane, round == 0);
   }
 }
 
-void launch_decide(const DecideArgs& a, cudaStream_t s) {
+// A batch's first boxes past their cut, one block a part (first_signs).
+__global__ void __launch_bounds__(256) k_first_signs_batch(DecideBatchArgs b) {
+  const int p = blockIdx.x;
+  first_signs(b.args[2 * p], int64_t(b.cnt[2 * p]));
+}
+
+void launch_decide(const DecideArgs& a, cudaStream_t s, bool first) {
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int64_t want = (a.n + DWARPS * 32 - 1) / (DWARPS * 32);
   const int grid = int(std::max<int64_t>(1, std::min<int64_t>(want, int64_t(sms) * 2)));
   k_decide_w<<<grid, DWARPS * 32, 0, s>>>(a);
+  if (first) k_first_signs<<<1, 256, 0, s>>>(a, a.n);
 }
 
 void launch_decide_batch(const DecideBatchArgs& b, int rounds, cudaStream_t s) {
@@ -232,6 +324,7 @@ void launch_decide_batch(const DecideBatchArgs& b, int rounds, cudaStream_t s) {
   for (int r = 0; r < rounds; r++) {
     k_decide_prep<<<1, 32, 0, s>>>(b, r);
     k_decide_batch<<<sms * 2, DWARPS * 32, 0, s>>>(b, r);
+    if (r == 0) k_first_signs_batch<<<b.n_parts, 256, 0, s>>>(b);
   }
 }
 

@@ -72,6 +72,11 @@ struct DecideArgs {
   double* read_dc;
   int64_t read_cap;
   unsigned long long* n_read;
+  // The first round's boxes lie on a grid of first_dims boxes (x fastest, in list
+  // order): their centres' values (NaN unless exact) and signs for k_first_signs.
+  double* first_sd;
+  int8_t* first_sign;
+  long long first_dims[3];
 };
 
 __global__ void k_points(DPack P, const double* xyz, int64_t n, double cap, double* value, int8_t* flag);
@@ -83,8 +88,9 @@ void launch_bricks(const BrickArgs& a, cudaStream_t s, int warps = 4);
 __global__ void k_assemble_batch(const int64_t* idx, const int32_t* part_of, const int64_t* part_off,
                                  uint32_t* const* maps, const int32_t* kind, const int64_t* slot, int64_t n,
                                  const uint32_t* words, uint32_t* atlas);
-// The decision of one box size of a level (decide.cu), 32 boxes a warp.
-void launch_decide(const DecideArgs& a, cudaStream_t s);
+// The decision of one box size of a level (decide.cu), 32 boxes a warp; `first`: the
+// level's first boxes, whose far ones then take their sign from a neighbour.
+void launch_decide(const DecideArgs& a, cudaStream_t s, bool first = false);
 
 // Many parts' decisions together (decide.cu), one round a box size. Part p's fields are
 // args[2p + (round & 1)]: `size` its first boxes' size (round r decides size >> r),

@@ -51,7 +51,7 @@ namespace icam {
 struct Box4;
 }
 // api.cu: the first boxes of a level's decision (their size in bricks returned).
-long long first_boxes(const LevelDesc& L, std::vector<icam::Box4>* out);
+long long first_boxes(const LevelDesc& L, std::vector<icam::Box4>* out, long long dims[3] = nullptr);
 
 struct IcamPack;
 // api.cu: the decision (partcache.rs:226-331) through the sort of the read bricks.
@@ -70,7 +70,7 @@ struct IcamPack {
     void* p = nullptr;
     size_t n = 0;
   };
-  Buf scratch[16];
+  Buf scratch[17];
   std::string err;
   unsigned long long* d_stats = nullptr;
   const uint32_t* last_map = nullptr;
