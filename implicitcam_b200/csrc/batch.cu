@@ -278,7 +278,7 @@ int icam_batch_bake(IcamBatch* bt, const IcamBatchLevel* levels, int precision, 
       (r = bbuf(bt, 14, LV * sizeof(uint32_t), &maps_all)) || (r = bbuf(bt, 15, LV * sizeof(int64_t), &ridx)) ||
       (r = bbuf(bt, 16, LV * sizeof(double), &rdc)) ||
       (r = bbuf(bt, 17, (3 * n + 2) * sizeof(unsigned long long), &cnt)) ||
-      (r = bbuf(bt, 18, (n + 1) * sizeof(int64_t), &groups)) || (r = bbuf(bt, 19, 2 * n * sizeof(DecideArgs), &d_args)) ||
+      (r = bbuf(bt, 18, (n + 2) * sizeof(int64_t), &groups)) || (r = bbuf(bt, 19, 2 * n * sizeof(DecideArgs), &d_args)) ||
       (r = bbuf(bt, 20, (n + 1) * sizeof(int64_t), &d_roff))) {
     cleanup();
     return r;

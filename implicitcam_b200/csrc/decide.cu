@@ -116,16 +116,17 @@ __device__ void decide_box(const DecideArgs& a, long long size, const Box4& b, d
   }
 }
 
-// 32 boxes of one size from boxes[g0 ..] (n in all): their centres' bounding ball, the
+// gs (1 to 32) boxes of one size from boxes[g0 ..] (n in all), a lane each: their
+// centres' bounding ball, the
 // features within its radius plus the cut of its centre (listed and ranked once,
 // sub-patches seeded there), every centre's value capped at the cut by the shared walk,
 // then each box decided.
 __device__ __forceinline__ void decide_group(const DecideArgs& a, const Box4* boxes, int64_t n, long long size,
-                                             int64_t g0, DecideSmem& S, int lane, bool first) {
+                                             int64_t g0, int gs, DecideSmem& S, int lane, bool first) {
   const DPack& P = a.P;
   const double side = 8.0 * a.h;
   const int64_t i = g0 + lane;
-  const bool live = i < n;
+  const bool live = lane < gs && i < n;
   const Box4 b = boxes[live ? i : g0];
   double3 lo = mk(a.lo[0] + side * b.x - a.clamp, a.lo[1] + side * b.y - a.clamp, a.lo[2] + side * b.z - a.clamp);
   double3 hi = mk(a.lo[0] + side * (b.x + size) + a.clamp, a.lo[1] + side * (b.y + size) + a.clamp,
@@ -255,11 +256,20 @@ __device__ void first_signs(const DecideArgs& a, int64_t n) {
 
 __global__ void __launch_bounds__(256) k_first_signs(DecideArgs a, int64_t n) { first_signs(a, n); }
 
-__global__ void __launch_bounds__(DWARPS * 32, 2) k_decide_w(DecideArgs a) {
+// The boxes a warp takes together: 32 when there are enough groups of 32 to fill the
+// GPU's warp slots (two 4-warp blocks an SM), else fewer (down to 4), so that a round of
+// few boxes (the first, of large boxes with long lists) spreads over more warps.
+__host__ __device__ inline int group_size(int64_t n, int sms) {
+  int gs = 32;
+  while (gs > 4 && n / gs < int64_t(sms) * 2 * DWARPS) gs /= 2;
+  return gs;
+}
+
+__global__ void __launch_bounds__(DWARPS * 32, 2) k_decide_w(DecideArgs a, int gs) {
   __shared__ DecideSmem smem[DWARPS];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int64_t g0 = (int64_t(blockIdx.x) * DWARPS + warp) * 32; g0 < a.n; g0 += int64_t(gridDim.x) * DWARPS * 32)
-    decide_group(a, a.boxes, a.n, a.size, g0, smem[warp], lane, a.first_sd != nullptr);
+  for (int64_t g0 = (int64_t(blockIdx.x) * DWARPS + warp) * gs; g0 < a.n; g0 += int64_t(gridDim.x) * DWARPS * gs)
+    decide_group(a, a.boxes, a.n, a.size, g0, gs, smem[warp], lane, a.first_sd != nullptr);
 }
 
 // A batch's round (one box size a part): the counts the last round appended become this
@@ -267,7 +277,7 @@ __global__ void __launch_bounds__(DWARPS * 32, 2) k_decide_w(DecideArgs a) {
 // One thread: a batch holds tens to thousands of parts.
 __global__ void k_decide_prep(DecideBatchArgs b, int round) {
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
-  int64_t g = 0;
+  int64_t total = 0;
   for (int p = 0; p < b.n_parts; p++) {
     unsigned long long* cur = b.cnt + 2 * p + (round & 1);
     unsigned long long* next = b.cnt + 2 * p + ((round + 1) & 1);
@@ -277,11 +287,18 @@ __global__ void k_decide_prep(DecideBatchArgs b, int round) {
       *cur = (unsigned long long)a.next_cap;
     }
     *next = 0;
-    b.boxes_read[0] += *cur;
+    total += int64_t(*cur);
+  }
+  const int gs = group_size(total, b.sms);
+  int64_t g = 0;
+  for (int p = 0; p < b.n_parts; p++) {
+    const unsigned long long cur = b.cnt[2 * p + (round & 1)];
+    b.boxes_read[0] += cur;
     b.groups[p] = g;
-    g += int64_t((*cur + 31) / 32);
+    g += int64_t((cur + gs - 1) / gs);
   }
   b.groups[b.n_parts] = g;
+  b.groups[b.n_parts + 1] = gs;
 }
 
 // A batch's round: every part's boxes of this round's size, 32 of one part a warp, the
@@ -290,6 +307,7 @@ __global__ void __launch_bounds__(DWARPS * 32, 2) k_decide_batch(DecideBatchArgs
   __shared__ DecideSmem smem[DWARPS];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t total = b.groups[b.n_parts];
+  const int gs = int(b.groups[b.n_parts + 1]);
   for (int64_t g = int64_t(blockIdx.x) * DWARPS + warp; g < total; g += int64_t(gridDim.x) * DWARPS) {
     int lo = 0, hi = b.n_parts;  // the part: groups[p] <= g < groups[p + 1]
     while (hi - lo > 1) {
@@ -299,7 +317,7 @@ __global__ void __launch_bounds__(DWARPS * 32, 2) k_decide_batch(DecideBatchArgs
     }
     const DecideArgs& a = b.args[2 * lo + (round & 1)];
     const int64_t n = int64_t(b.cnt[2 * lo + (round & 1)]);
-    decide_group(a, a.boxes, n, a.size >> round, (g - b.groups[lo]) * 32, smem[warp], lane, round == 0);
+    decide_group(a, a.boxes, n, a.size >> round, (g - b.groups[lo]) * gs, gs, smem[warp], lane, round == 0);
   }
 }
 
@@ -312,19 +330,22 @@ __global__ void __launch_bounds__(256) k_first_signs_batch(DecideBatchArgs b) {
 void launch_decide(const DecideArgs& a, cudaStream_t s, bool first) {
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int64_t want = (a.n + DWARPS * 32 - 1) / (DWARPS * 32);
+  const int gs = group_size(a.n, sms);
+  const int64_t want = (a.n + DWARPS * gs - 1) / (DWARPS * gs);
   const int grid = int(std::max<int64_t>(1, std::min<int64_t>(want, int64_t(sms) * 2)));
-  k_decide_w<<<grid, DWARPS * 32, 0, s>>>(a);
+  k_decide_w<<<grid, DWARPS * 32, 0, s>>>(a, gs);
   if (first) k_first_signs<<<1, 256, 0, s>>>(a, a.n);
 }
 
 void launch_decide_batch(const DecideBatchArgs& b, int rounds, cudaStream_t s) {
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  DecideBatchArgs bb = b;
+  bb.sms = sms;
   for (int r = 0; r < rounds; r++) {
-    k_decide_prep<<<1, 32, 0, s>>>(b, r);
-    k_decide_batch<<<sms * 2, DWARPS * 32, 0, s>>>(b, r);
-    if (r == 0) k_first_signs_batch<<<b.n_parts, 256, 0, s>>>(b);
+    k_decide_prep<<<1, 32, 0, s>>>(bb, r);
+    k_decide_batch<<<sms * 2, DWARPS * 32, 0, s>>>(bb, r);
+    if (r == 0) k_first_signs_batch<<<b.n_parts, 256, 0, s>>>(bb);
   }
 }
 

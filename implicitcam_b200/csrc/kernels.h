@@ -96,10 +96,12 @@ void launch_decide(const DecideArgs& a, cudaStream_t s, bool first = false);
 // args[2p + (round & 1)]: `size` its first boxes' size (round r decides size >> r),
 // boxes / next its two box regions (swapped between the pair), n_next its next count
 // (cnt[2p + ((round + 1) & 1)]), n_read its read count. cnt[2p] holds the first boxes'
-// count at the start; groups (n_parts + 1 values) is k_decide_prep's numbering.
+// count at the start; groups (n_parts + 2 values) is k_decide_prep's numbering and the
+// round's boxes a group.
 struct DecideBatchArgs {
   const DecideArgs* args;
   int n_parts;
+  int sms;  // the device's SMs (set by launch_decide_batch)
   unsigned long long* cnt;
   int64_t* groups;
   unsigned long long* boxes_read;
