@@ -28,9 +28,10 @@ static_assert(sizeof(DecideSmem) * DWARPS <= 48 * 1024, "static shared memory of
 
 // One box's verdict from its centre's value (v, f) read within `cut` (partcache.rs:370-383:
 // decided once the centre is known past the box grown by the clamp), the map entries it
-// settles, and its children (8 to a box, appended together) or its read.
+// settles, and its children (up to 8: into kids, *nk of them, for the caller to append;
+// appended here together when kids is null) or its read.
 __device__ void decide_box(const DecideArgs& a, long long size, const Box4& b, double3 c, double r, double cut,
-                           double v, int f) {
+                           double v, int f, Box4* kids_out = nullptr, int* nk_out = nullptr) {
   const DPack& P = a.P;
   const double side = 8.0 * a.h;
   double sd = NAN;  // the signed distance at the centre when known
@@ -109,6 +110,11 @@ __device__ void decide_box(const DecideArgs& a, long long size, const Box4& b, d
       }
       kids[nk++] = k;
     }
+    if (kids_out) {
+      for (int q = 0; q < nk; q++) kids_out[q] = kids[q];
+      *nk_out = nk;
+      return;
+    }
     // together, so that the next level's warps take neighbouring boxes
     unsigned long long slot = atomicAdd(a.n_next, (unsigned long long)nk);
     for (int q = 0; q < nk; q++)
@@ -170,6 +176,8 @@ __device__ __forceinline__ void decide_group(const DecideArgs& a, const Box4* bo
   double v;
   int f;
   warp_point<false>(P, W, c, gc, live, cut, lane, &v, &f);
+  Box4 kids[8];
+  int nk = 0;
   if (live) {
     if (first) {
       // a first box past its cut (air or material, its sign not known: it has no parent)
@@ -177,8 +185,22 @@ __device__ __forceinline__ void decide_group(const DecideArgs& a, const Box4* bo
       a.first_sd[i] = f == 0 ? v : NAN;
       a.first_sign[i] = f == 1 ? FS_PENDING : ((f == 0 && v != 0.0) ? (v > 0 ? 1 : -1) : 0);
     }
-    if (!(first && f == 1)) decide_box(a, size, b, c, r, cut, v, f);
+    if (!(first && f == 1)) decide_box(a, size, b, c, r, cut, v, f, kids, &nk);
   }
+  // the group's children appended together, in lane order, so that the next round's
+  // groups take neighbouring boxes (a group's boxes are neighbours, their children too)
+  int incl = nk;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(FULL, incl, o);
+    if (lane >= o) incl += t;
+  }
+  const int total = __shfl_sync(FULL, incl, 31);
+  unsigned long long base = 0;
+  if (lane == 31 && total > 0) base = atomicAdd(a.n_next, (unsigned long long)total);
+  base = __shfl_sync(FULL, base, 31);
+  const unsigned long long off = base + (unsigned long long)(incl - nk);
+  for (int q = 0; q < nk; q++)
+    if (off + q < (unsigned long long)a.next_cap) a.next[off + q] = kids[q];
   __syncwarp();
 }
 
