@@ -78,6 +78,22 @@ def workload(seed: int, kind: str = "freeform"):
     return b, lo, nb
 
 
+def over_ranks(dist, device, ms, voxels=None):
+    """The job's figures over the ranks: the slowest rank's time (max) and every rank's
+    voxels (sum); as given on one process. Every rank calls it at the same point."""
+    if dist is None:
+        return ms, voxels
+    import torch
+
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    if voxels is None:
+        return float(t.item()), None
+    v = torch.tensor([voxels], device=device, dtype=torch.float64)
+    dist.all_reduce(v)
+    return float(t.item()), float(v.item())
+
+
 def workload_name(kind):
     if kind == "mold":
         return f"mold cavity pocket level bake (500 B-spline floor faces), h={H} mm, band +-{BAND} mm"
@@ -251,14 +267,8 @@ def main():
             ms.append(t)
             stats.append(st)
         torch.cuda.synchronize()
-        total_ms, voxels = float(sum(ms)), 512.0 * stats[-1]["bricks_read"]
+        total_ms, voxels = over_ranks(dist, f"cuda:{local}", float(sum(ms)), 512.0 * stats[-1]["bricks_read"])
         if dist:
-            t = torch.tensor([total_ms], device=f"cuda:{local}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            total_ms = float(t.item())
-            v = torch.tensor([voxels], device=f"cuda:{local}", dtype=torch.float64)
-            dist.all_reduce(v)
-            voxels = float(v.item())
             dist.barrier()
         return total_ms, voxels, stats
 
@@ -282,11 +292,7 @@ def main():
     for _ in range(max(1, args.steps)):
         t, ns, st = step(prec, device_only=False, host=(m_host, a_host))
         e2e_ms.append(t)
-    e2e_total = float(sum(e2e_ms))
-    if dist:
-        t = torch.tensor([e2e_total], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_total = float(t.item())
+    e2e_total, _ = over_ranks(dist, f"cuda:{local}", float(sum(e2e_ms)))
     e2e_value = voxels * len(e2e_ms) / (e2e_total * 1e-3)
     d2h = int(np.prod(nb)) * 4 + stats[-1]["bricks_words"] * part_gpu.WORDS * 4
     error = None
