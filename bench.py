@@ -197,9 +197,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--h", type=float, default=None, help="cell side (mm); smaller cases for profiling")
     ap.add_argument("--band", type=float, default=None, help="narrow band half-width (mm), the clamp")
-    ap.add_argument("--workload", default="freeform", choices=["freeform", "batch", "mold"],
+    ap.add_argument("--workload", default="freeform", choices=["freeform", "batch", "mold", "block"],
                     help="freeform: the headline (h 0.1 mm, band 2 mm); mold: the mold cavity's pocket "
-                         "(h 0.05 mm, band 1 mm); batch: 64 seeded uneven parts at h = 0.2 mm baked together")
+                         "(h 0.05 mm, band 1 mm); batch: 64 seeded uneven parts at h = 0.2 mm baked together; "
+                         "block: the block with a hole's point queries and levels")
     ap.add_argument("--seednet-steps", type=int, default=SEEDNET_STEPS,
                     help="training steps of the seed network (fewer only for profiling captures)")
     args = ap.parse_args()
@@ -212,6 +213,8 @@ def main():
         return run_reference(args, rank, world)
     if args.workload == "batch":
         return run_batch(args, rank, world)
+    if args.workload == "block":
+        return run_block(args, rank, world)
 
     import torch
 
@@ -436,6 +439,88 @@ def run_batch(args, rank, world):
     batch.close()
     for g in gs:
         g.close()
+
+
+def run_block(args, rank, world):
+    """The block with a hole (100 x 60 x 40 mm minus a 20 mm hole): 10^6 point queries
+    uniform over the box grown by 10 mm (the reference checker's generator, seed 0)
+    through icam_points, and the level over the part's box from (0, 0, 0) at h = 0.5 mm
+    (25 x 15 x 10 bricks) and h = 1 mm, clamp a cell's diagonal; the oracle on the host's
+    cores beside them. One process (the part is small)."""
+    import torch
+
+    from implicitcam_b200 import part_gpu, parts
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import icam_oracle
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+    prec = {"fp64": part_gpu.FP64, "mixed": part_gpu.MIXED, "learned": part_gpu.MIXED}[args.precision]
+    b = parts.block_with_hole()
+    g = part_gpu.PartGpu(b)
+    rng = parts.Rng(0)
+    n = 1_000_000
+    lo_q, hi_q = np.array([-10.0, -10.0, -10.0]), np.array([110.0, 70.0, 50.0])
+    q = np.array([[rng.uniform(lo_q[k], hi_q[k]) for k in range(3)] for _ in range(n)])
+    stream = torch.cuda.ExternalStream(g.stream())
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def timed(fn):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1), out
+
+    for _ in range(args.warmup):
+        g.points(q[:100000], precision=prec)
+    ms = [timed(lambda: g.points(q, precision=prec))[0] for _ in range(args.steps)]
+    q_per_s = n / (np.mean(ms) * 1e-3)
+    bakes = {}
+    for h in (0.5, 1.0):
+        nb = np.ceil(np.array([100.0, 60.0, 40.0]) / (8 * h)).astype(np.int64)
+        lo = np.zeros(3)
+        for _ in range(args.warmup):
+            g.level_device(h, lo, nb, precision=prec)
+        res = [timed(lambda: g.level_device(h, lo, nb, precision=prec)) for _ in range(args.steps)]
+        t = float(np.mean([r[0] for r in res]))
+        st = res[-1][1][3]
+        bakes[f"h{h}"] = {"nb": nb.tolist(), "bricks": int(np.prod(nb)), "bricks_read": st["bricks_read"],
+                          "bricks_stored": st["bricks_words"], "ms": t,
+                          "voxels_per_s": 512.0 * st["bricks_read"] / (t * 1e-3),
+                          "level_cells_per_s": 512.0 * float(np.prod(nb)) / (t * 1e-3)}
+    o = icam_oracle.Oracle(b)
+    sample = q[:: n // 20000]
+    t0 = time.perf_counter()
+    o.sdf(sample)
+    cpu_q = len(sample) / (time.perf_counter() - t0)
+    nb1 = np.ceil(np.array([100.0, 60.0, 40.0]) / 8.0).astype(np.int64)
+    t0 = time.perf_counter()
+    om, idx, dc = o.decide(1.0, np.zeros(3), nb1, np.sqrt(3.0))
+    firsts = np.stack([8.0 * (idx % nb1[0]), 8.0 * ((idx // nb1[0]) % nb1[1]), 8.0 * (idx // (nb1[0] * nb1[1]))], 1)
+    o.bricks(firsts.astype(np.float64), 1.0, np.sqrt(3.0))
+    cpu_bake = time.perf_counter() - t0
+    if rank == 0:
+        print(json.dumps({
+            "metric": "block with hole: exact signed-distance point queries/s (end to end through icam_points)",
+            "value": q_per_s, "unit": "queries/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": float(np.mean(ms)), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if prec == part_gpu.FP64 else "f32+f64", "data": "synthetic",
+            "config": {"workload": "block 100x60x40 mm minus a 20 mm hole: 1e6 uniform queries over the box "
+                                   "grown by 10 mm (seed 0), levels at h 0.5 and 1 mm", "precision": args.precision,
+                       "l2": "flushed (256 MB write) before every step"},
+            "e2e": {"value": q_per_s, "unit": "queries/s", "h2d_bytes_per_step": n * 24,
+                    "d2h_bytes_per_step": n * 9},
+            "bakes": bakes,
+            "cpu_baseline": {"queries_per_s": cpu_q, "cores": o.threads, "kind": "port",
+                             "sample": f"{len(sample)} of the queries; the h = 1 mm level (decision and every read "
+                                       f"brick) in {cpu_bake:.2f} s",
+                             "level_h1_s": cpu_bake},
+        }), flush=True)
+    g.close()
 
 
 def compare_with_fp64(g, part_gpu, prec, lo, nb, m_arm, a_arm):
