@@ -253,6 +253,7 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 2) k_bricks_t(BrickArgs a) {
     __syncwarp();
     // ---- 3. every node: the warp's lanes walk the same ranked candidates together
     int cnt[3] = {0, 0, 0};
+    int pending = 0;
     const WarpCands W{S.code, S.lb, S.cert, S.slot, S.v.seed, S.net, S.net32, n, overflow};
     for (int nn0 = 0; nn0 < 729; nn0 += 32) {
       const int nn = nn0 + lane;
@@ -260,15 +261,37 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 2) k_bricks_t(BrickArgs a) {
       double3 p = first + mk(h * (nn % 9), h * ((nn / 9) % 9), h * (nn / 81));
       double v;
       int f;
-      warp_point<MIXED>(P, W, p, c, live, clamp, lane, &v, &f);
+      warp_point<MIXED, false>(P, W, p, c, live, clamp, lane, &v, &f);
       if (!live) continue;
+      S.flag[nn] = int8_t(f);
+      if (f == 3) {
+        pending++;
+        continue;
+      }
       if (a.d_out) a.d_out[bi * 729 + nn] = v;
       if (a.flag_out) a.flag_out[bi * 729 + nn] = int8_t(f);
-      S.flag[nn] = int8_t(f);
       S.u.f[nn] = f == 0 ? v : NAN;
       cnt[f]++;
     }
     __syncwarp();
+    // the nodes the list left undecided (rare: a feature whose certificate failed there,
+    // or more candidates than the list holds): the whole tree walk, a lane a node, kept
+    // out of the loop above so that its code stays small
+    if (__any_sync(FULL, pending > 0)) {
+      for (int nn = lane; nn < 729; nn += 32) {
+        if (S.flag[nn] != 3) continue;
+        double3 p = first + mk(h * (nn % 9), h * ((nn / 9) % 9), h * (nn / 81));
+        double v;
+        int f;
+        point_fallback(P, p, clamp, &v, &f);
+        if (a.d_out) a.d_out[bi * 729 + nn] = v;
+        if (a.flag_out) a.flag_out[bi * 729 + nn] = int8_t(f);
+        S.flag[nn] = int8_t(f);
+        S.u.f[nn] = f == 0 ? v : NAN;
+        cnt[f]++;
+      }
+      __syncwarp();
+    }
     const int n_exact = __reduce_add_sync(FULL, cnt[0]), n_far = __reduce_add_sync(FULL, cnt[1]),
               n_und = __reduce_add_sync(FULL, cnt[2]);
     int provisional = 0;

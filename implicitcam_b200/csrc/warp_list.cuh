@@ -233,7 +233,7 @@ struct WarpCands {
 // point is nearer than the next bound. MIXED: sub-patches run Newton in floats on the
 // rebased nets and are polished in doubles, with the critical-point test and the trim,
 // only when their float distance can beat the answer so far.
-template <bool MIXED>
+template <bool MIXED, bool TAIL = true>
 __device__ __forceinline__ void warp_point(const DPack& P, const WarpCands& W, double3 p, double3 c, bool live,
                                            double cap, int lane, double* value, int* flag) {
   const double rr = len(p - c);
@@ -342,6 +342,12 @@ __device__ __forceinline__ void warp_point(const DPack& P, const WarpCands& W, d
     if (got == 2) defer_item(code, lb);
   }
   if (!live) return;
+  // !TAIL: a point the list leaves undecided is handed back (flag 3) for the caller to
+  // read by the whole tree walk later, out of the loop that calls this one
+  if (!TAIL && (W.overflow || (und < best && und <= cap))) {
+    *value = NAN, *flag = 3;
+    return;
+  }
   if (nd > 0 && nd <= 2 && und < best && und <= cap) point_resolve(P, p, dc0, dl0, dc1, dl1, nd, &best, &sdv, &und);
   if (W.overflow || (und < best && und <= cap)) {
     point_fallback(P, p, cap, value, flag);
