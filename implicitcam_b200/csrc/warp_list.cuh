@@ -81,7 +81,10 @@ __device__ __forceinline__ int warp_list(const DPack& P, const int32_t* leaves, 
     }
   }
   __syncwarp();
-  return *count;
+  // every lane reads the count before any lane may go on to reset it (a next list)
+  const int n = *count;
+  __syncwarp();
+  return n;
 }
 
 // The first n of tcode / tlb ranked by bound into code / lb, ties by code so the order
