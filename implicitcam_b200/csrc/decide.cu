@@ -11,17 +11,21 @@ constexpr int DWARPS = 4;  // box groups a block works on at once, one a warp
 // surface), pending (past its cut, sign not known), then air or material once known
 constexpr int8_t FS_PENDING = 2, FS_AIR = 3, FS_SOLID = -3;
 
+// A box group's list holds twice a brick's candidates: a box's cut reaches farther, and
+// a list that overflows sends every lane to walk the tree alone.
+constexpr int DMAXC = 2 * MAXC;
+
 struct DecideSmem {
-  uint32_t tcode[MAXC];  // the list before its ranking, and the walk's frontier
-  double tlb[MAXC];
+  uint32_t tcode[DMAXC];  // the list before its ranking, and the walk's frontier
+  double tlb[DMAXC];
   int32_t fr[2][FR];
-  double lb[MAXC];  // ranked candidates
-  uint32_t code[MAXC];
+  double lb[DMAXC];  // ranked candidates
+  uint32_t code[DMAXC];
   Seed seed[MAXSUB];
   double4 net[16];
   float4 net32[16];
-  int8_t cert[MAXC];
-  int8_t slot[MAXC];
+  int8_t cert[DMAXC];
+  int8_t slot[DMAXC];
   int n;
 };
 static_assert(sizeof(DecideSmem) * DWARPS <= 48 * 1024, "static shared memory of a block");
@@ -151,9 +155,9 @@ __device__ __forceinline__ void decide_group(const DecideArgs& a, const Box4* bo
   double R = len(c - gc);
   for (int o = 16; o > 0; o >>= 1) R = fmax(R, __shfl_xor_sync(FULL, R, o));
   // every feature nearer than the cut to a centre has a bound <= R + cut from gc
-  int nc = warp_list(P, a.leaves, a.n_leaves, gc, R + cut, S.tcode, S.tlb, S.fr, &S.n, lane);
-  const bool overflow = nc > MAXC;
-  if (overflow) nc = MAXC;
+  int nc = warp_list<DMAXC>(P, a.leaves, a.n_leaves, gc, R + cut, S.tcode, S.tlb, S.fr, &S.n, lane);
+  const bool overflow = nc > DMAXC;
+  if (overflow) nc = DMAXC;
   warp_rank(S.tcode, S.tlb, nc, S.code, S.lb, lane);
   int subs_before = 0;
   for (int base = 0; base < nc; base += 32) {

@@ -14,9 +14,10 @@ constexpr int FR = 64;      // tree nodes one level of the list's walk may hold
 constexpr int MAXSUB = 32;  // sub-patches seeded from the centre
 
 // The features with a lower bound <= reach from c, unranked into tcode / tlb (at most
-// MAXC kept; the count returned may exceed it). The tree is walked a level at a time,
+// CAP kept; the count returned may exceed it). The tree is walked a level at a time,
 // a lane a node; a level wider than the frontier gives way to every leaf in turn.
 // *count is a shared counter of the warp; fr two frontier buffers of FR nodes.
+template <int CAP = MAXC>
 __device__ __forceinline__ int warp_list(const DPack& P, const int32_t* leaves, int n_leaves, double3 c, double reach,
                                          uint32_t* tcode, double* tlb, int32_t (*fr)[FR], int* count, int lane) {
   auto take_leaf = [&](const DBvh& nd) {
@@ -25,7 +26,7 @@ __device__ __forceinline__ int warp_list(const DPack& P, const int32_t* leaves, 
       double lb = item_lb(P, code, c);
       if (lb <= reach) {
         int slot = atomicAdd(count, 1);
-        if (slot < MAXC) {
+        if (slot < CAP) {
           tcode[slot] = code;
           tlb[slot] = lb;
         }
