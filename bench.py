@@ -43,9 +43,9 @@ BAND = 2.0
 # leg; 6 Newton steps of 750 + trim 200; closed-form foot; 6 steps of 120; a distance
 FLOPS_PER_CANDIDATE = np.array([80.0, 6 * 750.0 + 200.0, 40.0, 6 * 120.0, 10.0])
 # DRAM bytes k_bricks moves a read brick: one ncu capture of the same kernel (mixed form)
-# on a level 7x smaller (profiles/k_bricks_freeform_h0.2.md: 3.69 GB/s x 34.95 ms =
-# 128.9 MB over 129,053 read bricks), scaled by the bricks read
-TRAFFIC_PER_READ_BRICK = 3.68694e9 * 34.95328e-3 / 129053
+# on a level 7x smaller (profiles/k_bricks_freeform_h0.2.md: 8.55 GB/s x 13.06 ms =
+# 111.7 MB over 129,053 read bricks), scaled by the bricks read
+TRAFFIC_PER_READ_BRICK = 8.551313e9 * 13.0616e-3 / 129053
 # the seed network's training: 50M pairs from the exact evaluator, before any timing
 SEEDNET_STEPS, SEEDNET_BATCH = 12208, 4096
 
