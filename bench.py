@@ -13,8 +13,9 @@ own part (seed = rank): weak scaling, no collective on the data path.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--precision learned|mixed|fp64]
 
 The headline arm (default: mixed precision with the seed network's Newton starts) is
-timed beside the plain FP64 kernel on the same level; the line carries both, the
-speed-up, and the headline's error against FP64 (map, signs, i16 words, distances).
+timed beside the plain FP64 kernel and the mixed form without the network on the same
+level; the line carries all three, the speed-up over FP64, and the headline level's
+error against the f64 oracle (its decision whole, sampled nodes and distances).
     python bench.py --impl reference ...   # the reference's CPU path (the oracle port)
 
 Prints one JSON line (rank 0).
@@ -43,8 +44,8 @@ BAND = 2.0
 # leg; 6 Newton steps of 750 + trim 200; closed-form foot; 6 steps of 120; a distance
 FLOPS_PER_CANDIDATE = np.array([80.0, 6 * 750.0 + 200.0, 40.0, 6 * 120.0, 10.0])
 # DRAM bytes k_bricks moves a read brick: one ncu capture of the same kernel (mixed form)
-# on a level 7x smaller (profiles/k_bricks_freeform_h0.2.md: 8.55 GB/s x 13.06 ms =
-# 111.7 MB over 129,053 read bricks), scaled by the bricks read
+# on the same part's level at h = 0.2 mm, 7x smaller (8.55 GB/s x 13.06 ms = 111.7 MB
+# over 129,053 read bricks), scaled by the bricks read
 TRAFFIC_PER_READ_BRICK = 8.551313e9 * 13.0616e-3 / 129053
 # the seed network's training: 50M pairs from the exact evaluator, before any timing
 SEEDNET_STEPS, SEEDNET_BATCH = 12208, 4096
@@ -132,47 +133,75 @@ def read_clocks(path, device):
             "samples": len(sm)}
 
 
-def cpu_bake_sample(seed, bricks_target_s=12.0, threads=None, kind="freeform"):
-    """The oracle's bake (the reference's exact_brick, partcache.rs:979) of a sample of
-    the level's read bricks on all host cores: voxels/s, cores, sample text."""
+def cpu_level_sample(seed, kind="freeform", target_s=8.0, threads=None, region=16):
+    """The reference's CPU bake of the level (PartCache::level on the exact source:
+    decide, then exact_brick for every brick to read; partcache.rs:226-331, 979-1058) as
+    the oracle restates it, timed on all host cores over a random sample of the level.
+    The level is cut into regions of region^3 bricks on its box grid; a region whose
+    centre lies farther from the surface than its half-diagonal plus twice the band
+    holds no brick to read. Regions are drawn at random from both kinds, near first,
+    until target_s of CPU time is spent; in each, the oracle's decision is timed whole
+    and exact_brick over up to 24 of its bricks to read, drawn uniformly; each kind's
+    time and bricks to read are extrapolated to all regions of that kind. Voxels are
+    counted as the GPU arm counts them: 512 for every brick the decision reads.
+    Returns (voxels/s, cores, sample text)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import icam_oracle
 
     b, lo, nb = workload(seed, kind)
     o = icam_oracle.Oracle(b, threads=threads)
-    rng = np.random.default_rng(seed)
-    # bricks the bake reads: those holding random points of the B-spline spans (every
-    # brick the surface passes through is read)
-    pa = np.concatenate([np.asarray(p).reshape(-1, 4, 4, 4) for p in b.patches])
-    k = 4096
-    ia = rng.integers(0, len(pa), k)
-    s, t = rng.uniform(0, 1, k), rng.uniform(0, 1, k)
-    bs = np.stack([(1 - s) ** 3, 3 * (1 - s) ** 2 * s, 3 * (1 - s) * s * s, s ** 3], 1)
-    bt = np.stack([(1 - t) ** 3, 3 * (1 - t) ** 2 * t, 3 * (1 - t) * t * t, t ** 3], 1)
-    hom = np.einsum("ki,kj,kijc->kc", bs, bt, pa[ia])
-    xyz = hom[:, :3] / hom[:, 3:]
-    cell = np.floor((xyz - lo) / (8 * H)).astype(np.int64)
-    firsts = lo + 8 * H * np.unique(cell, axis=0)
-    firsts = firsts[rng.permutation(len(firsts))]
-    n = 8
-    t0 = time.perf_counter()
-    o.bricks(firsts[:n], H, BAND)
-    dt = time.perf_counter() - t0
-    n2 = int(max(n, min(len(firsts), n * bricks_target_s / max(dt, 1e-3))))
-    t0 = time.perf_counter()
-    o.bricks(firsts[:n2], H, BAND)
-    dt = time.perf_counter() - t0
-    return 512.0 * n2 / dt, o.threads, f"{n2} random read bricks through the B-spline spans (h={H}, clamp={BAND}), {dt:.1f} s"
+    rng = np.random.default_rng(seed + 1)
+    nr = -(-nb // region)
+    grid = np.stack(np.meshgrid(*[np.arange(k) for k in nr], indexing="ij"), -1).reshape(-1, 3)
+    side = 8 * H * region
+    centres = lo + side * (grid + 0.5)
+    dcen = o.sdf(centres)[0]
+    near = np.abs(dcen) <= 0.5 * side * np.sqrt(3.0) + 2 * BAND
+    strata = {"near": rng.permutation(np.nonzero(near)[0]), "far": rng.permutation(np.nonzero(~near)[0])}
+    acc = {k: [0.0, 0.0, 0] for k in strata}  # seconds, bricks to read, regions
+    origin = lo + H  # the level's box grid (the oracle's default for the whole level)
+    spent, turn = 0.0, 0
+    t_start = time.perf_counter()
+    while spent < target_s and any(acc[k][2] < len(strata[k]) for k in strata):
+        k = "near" if (turn % 3 != 2 and acc["near"][2] < len(strata["near"])) or acc["far"][2] >= len(strata["far"]) else "far"
+        turn += 1
+        r = strata[k][acc[k][2]]
+        lo_r = lo + side * grid[r]
+        nb_r = np.minimum(region, nb - region * grid[r]).astype(np.int64)
+        t0 = time.perf_counter()
+        _, idx, _ = o.decide(H, lo_r, nb_r, BAND, origin=origin)
+        t_dec = time.perf_counter() - t0
+        t_brk = 0.0
+        if len(idx):
+            pick = rng.choice(idx, min(24, len(idx)), replace=False)
+            firsts = lo_r + 8 * H * np.stack([pick % nb_r[0], (pick // nb_r[0]) % nb_r[1],
+                                              pick // (nb_r[0] * nb_r[1])], 1)
+            t0 = time.perf_counter()
+            o.bricks(firsts, H, BAND)
+            t_brk = (time.perf_counter() - t0) * len(idx) / len(pick)
+        acc[k][0] += t_dec + t_brk
+        acc[k][1] += len(idx)
+        acc[k][2] += 1
+        spent = time.perf_counter() - t_start
+    T = sum(len(strata[k]) / a[2] * a[0] for k, a in acc.items() if a[2])
+    R = sum(len(strata[k]) / a[2] * a[1] for k, a in acc.items() if a[2])
+    text = (f"oracle decide + exact_brick over random {region}^3-brick regions of the level (h={H}, band={BAND}): "
+            f"{acc['near'][2]} of {len(strata['near'])} near the surface, {acc['far'][2]} of {len(strata['far'])} "
+            f"away from it, up to 24 bricks to read timed in each, extrapolated per region ({spent:.1f} s; "
+            f"estimated {T:.0f} s for the level's ~{R:.0f} bricks to read)")
+    return 512.0 * R / T, o.threads, text
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return
     vals = []
+    per_step = max(2.0, min(8.0, 100.0 / max(1, args.steps + args.warmup)))
     for _ in range(args.warmup):
-        cpu_bake_sample(0, bricks_target_s=2.0, kind=args.workload)
+        cpu_level_sample(0, kind=args.workload, target_s=per_step)
+    sample = ""
     for _ in range(args.steps):
-        v, cores, sample = cpu_bake_sample(0, bricks_target_s=8.0, kind=args.workload)
+        v, cores, sample = cpu_level_sample(0, kind=args.workload, target_s=per_step)
         vals.append(v)
     value = float(np.mean(vals))
     out = {
@@ -180,7 +209,8 @@ def run_reference(args, rank, world):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": workload_name(args.workload), "seed": 0},
-        "cpu_baseline": {"value": value, "unit": "voxels/s", "cores": cores, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": "voxels/s", "cores": cores, "kind": "port",
+                         "sample": f"each step: {sample}"},
         "e2e": {"value": value, "unit": "voxels/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out), flush=True)
@@ -278,12 +308,17 @@ def main():
     clk_path = os.path.join(tempfile.gettempdir(), f"icam_clocks_{os.getpid()}.csv")
     smi = sample_clocks(clk_path) if rank == 0 else None
     total_ms, voxels, stats = arm(prec)
-    fp64 = None
-    if prec != part_gpu.FP64:
-        f_ms, f_vox, f_stats = arm(part_gpu.FP64)
-        fp64 = {"value": f_vox * args.steps / (f_ms * 1e-3), "ms_per_step": f_ms / args.steps,
-                "stage_ms": {"decide": f_stats[-1]["ms_decide"], "nodes": f_stats[-1]["ms_nodes"],
-                             "assemble": f_stats[-1]["ms_post"]}}
+    # the other arms on the same level: the plain FP64 kernel (the metric's reference) and,
+    # beside the learned arm, the mixed form without the seed network (what the net gains)
+    others = {}
+    for name, p in (("fp64", part_gpu.FP64), ("mixed", part_gpu.MIXED)):
+        if p == prec or (name == "mixed" and prec != part_gpu.MIXED_LEARNED):
+            continue
+        o_ms, o_vox, o_stats = arm(p)
+        others[name] = {"value": o_vox * args.steps / (o_ms * 1e-3), "ms_per_step": o_ms / args.steps,
+                        "stage_ms": {"decide": float(np.mean([x["ms_decide"] for x in o_stats])),
+                                     "nodes": float(np.mean([x["ms_nodes"] for x in o_stats])),
+                                     "assemble": float(np.mean([x["ms_post"] for x in o_stats]))}}
     if smi:
         smi.terminate()
         smi.wait()
@@ -293,14 +328,27 @@ def main():
     a_host = torch.empty((max(stats[-1]["bricks_words"], 1) * part_gpu.WORDS,), dtype=torch.int32, pin_memory=True)
     e2e_ms = []
     for _ in range(max(1, args.steps)):
-        t, ns, st = step(prec, device_only=False, host=(m_host, a_host))
+        t, ns, st_e = step(prec, device_only=False, host=(m_host, a_host))
         e2e_ms.append(t)
     e2e_total, _ = over_ranks(dist, f"cuda:{local}", float(sum(e2e_ms)))
     e2e_value = voxels * len(e2e_ms) / (e2e_total * 1e-3)
-    d2h = int(np.prod(nb)) * 4 + stats[-1]["bricks_words"] * part_gpu.WORDS * 4
+    m_arm = m_host.numpy().view(np.uint32).copy()
+    a_arm = a_host.numpy().view(np.uint32)[: ns * part_gpu.WORDS].reshape(-1, part_gpu.WORDS).copy()
     error = None
-    if fp64 is not None:
-        error = compare_with_fp64(g, part_gpu, prec, lo, nb, m_host.numpy().copy(), a_host.numpy().copy())
+    if rank == 0 and not args.no_cpu:
+        # the checker (outside every timed region): the headline arm's level against the
+        # f64 oracle, with the oracle's own decision of the whole level
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import icam_oracle
+
+        t0 = time.perf_counter()
+        orc = icam_oracle.Oracle(b)
+        om, _, _ = orc.decide(H, lo, nb, BAND)
+        error = verify_against_oracle(g, orc, part_gpu, lo, nb, H, BAND, prec, m_arm, a_arm, decision=om)
+        if prec != part_gpu.FP64:
+            m64, _, _ = g.level(H, lo, nb, BAND, precision=part_gpu.FP64, atlas=False)
+            error["map_equal_to_fp64_kernel"] = bool((m64 == m_arm).all())
+        error["check_s"] = time.perf_counter() - t0
     if rank == 0:
         st = stats[-1]
         node_ms = float(np.mean([s["ms_nodes"] for s in stats]))
@@ -310,7 +358,7 @@ def main():
         achieved = flops / (node_ms * 1e-3)
         cpu = None
         if not args.no_cpu and world == 1:
-            v, cores, sample = cpu_bake_sample(0, kind=args.workload)
+            v, cores, sample = cpu_level_sample(0, kind=args.workload, target_s=12.0)
             cpu = {"value": v, "unit": "voxels/s", "cores": cores, "kind": "port", "sample": sample}
         clocks = read_clocks(clk_path, local)
         out = {
@@ -322,16 +370,16 @@ def main():
                        "part": "mold" if args.workload == "mold" else "freeform_top",
                        "seed": "rank", "h_mm": H, "band_mm": BAND, "nb": nb.tolist(), "precision": args.precision,
                        "l2": "flushed (256 MB write) before every step"},
-            "speedup_vs_fp64": None if fp64 is None else value / fp64["value"],
-            "fp64": fp64, "error_vs_fp64": error, "seednet": seednet,
+            "speedup_vs_fp64": value / others["fp64"]["value"] if "fp64" in others else None,
+            "fp64": others.get("fp64"), "mixed": others.get("mixed"), "error_vs_oracle": error, "seednet": seednet,
             "bricks_read": st["bricks_read"], "bricks_stored": st["bricks_words"],
             "bricks_settled": st["bricks_settled"],
             "nodes_exact": st["nodes_exact"], "nodes_undecided": st["nodes_undecided"],
             "nodes_exact_per_s": st["nodes_exact"] * args.steps / (total_ms * 1e-3),
             "stage_ms": {"decide": st["ms_decide"], "nodes": st["ms_nodes"], "assemble": st["ms_post"]},
             "gpu_launches": int(st["kernel_launches"]) * args.steps,
-            "e2e": {"value": e2e_value, "unit": "voxels/s", "h2d_bytes_per_step": 512,
-                    "d2h_bytes_per_step": d2h},
+            "e2e": {"value": e2e_value, "unit": "voxels/s", "h2d_bytes_per_step": st_e["h2d_bytes"],
+                    "d2h_bytes_per_step": st_e["d2h_bytes"]},
             "roofline": {"bound": "fp64" if prec == part_gpu.FP64 else "fp32", "kernel": "k_bricks",
                          "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": TRAFFIC_PER_READ_BRICK * st["bricks_read"],
@@ -476,8 +524,8 @@ def run_block(args, rank, world):
         return e0.elapsed_time(e1), out
 
     for _ in range(args.warmup):
-        g.points(q[:100000], precision=prec)
-    ms = [timed(lambda: g.points(q, precision=prec))[0] for _ in range(args.steps)]
+        g.points(q[:100000])
+    ms = [timed(lambda: g.points(q))[0] for _ in range(args.steps)]
     q_per_s = n / (np.mean(ms) * 1e-3)
     bakes = {}
     for h in (0.5, 1.0):
@@ -523,29 +571,91 @@ def run_block(args, rank, world):
     g.close()
 
 
-def compare_with_fp64(g, part_gpu, prec, lo, nb, m_arm, a_arm):
-    """The headline arm's level against the plain FP64 kernel's: the map (active set and
-    AIR / SOLID signs) equal, the i16 words' largest difference and sign flips, and the
-    largest distance difference over the diagonal on a sample of stored bricks."""
-    m64, a64, _ = g.level(H, lo, nb, BAND, precision=part_gpu.FP64)
-    m_arm = m_arm.view(np.uint32)[: len(m64)]
-    same_map = bool((m_arm == m64).all())
-    q64 = part_gpu.unpack_atlas(a64).astype(np.int64)
-    qa = part_gpu.unpack_atlas(a_arm.view(np.uint32)[: a64.size]).astype(np.int64)
-    flips = int(((q64 > 0) & (qa < 0)).sum() + ((q64 < 0) & (qa > 0)).sum())
-    stored = np.nonzero(m64 < 0xFFFFFFF0)[0]
-    rng = np.random.default_rng(0)
-    pick = stored[rng.permutation(len(stored))[:256]]
-    idx = np.stack([pick % nb[0], (pick // nb[0]) % nb[1], pick // (nb[0] * nb[1])], 1)
-    firsts = lo + 8 * H * idx
-    _, d64 = g.bricks(firsts, H, BAND, precision=part_gpu.FP64)
-    _, da = g.bricks(firsts, H, BAND, precision=prec)
-    diag = float(np.linalg.norm(np.asarray(nb) * 8 * H - 2 * BAND))  # the part's box, about
-    ok = (np.abs(d64) < BAND) & (np.abs(da) < BAND)
-    return {"map_equal": same_map, "i16_max_step_diff": int(np.abs(q64 - qa).max()) if q64.size else 0,
-            "sign_flips": flips, "max_abs_mm": float(np.abs(d64 - da)[ok].max()) if ok.any() else 0.0,
-            "max_over_diag": float(np.abs(d64 - da)[ok].max() / diag) if ok.any() else 0.0,
-            "sample": f"{len(pick)} stored bricks, every node within the band"}
+def brick_firsts(ids, lo, nb, h):
+    """First nodes of bricks given by level index (x fastest)."""
+    ids = np.asarray(ids, dtype=np.int64)
+    return np.stack([lo[0] + 8 * h * (ids % nb[0]), lo[1] + 8 * h * ((ids // nb[0]) % nb[1]),
+                     lo[2] + 8 * h * (ids // (nb[0] * nb[1]))], 1)
+
+
+def node_points(ids, nodes, lo, nb, h):
+    """Positions of nodes (0..728, x fastest) of bricks given by level index."""
+    f = brick_firsts(ids, lo, nb, h)
+    nodes = np.asarray(nodes, dtype=np.int64)
+    return f + h * np.stack([nodes % 9, (nodes // 9) % 9, nodes // 81], 1)
+
+
+def verify_against_oracle(g, oracle, part_gpu, lo, nb, h, clamp, precision, m, a, n_bricks=1000, every=29,
+                          n_centres=300, seed=0, decision=None):
+    """A baked level against the f64 oracle, as the reference's PartCache::verify does
+    it (partcache.rs:508-543; every 29th node, icam-sim main.rs:959): every `every`th
+    node of n_bricks random stored bricks, plus every node of every stored brick whose
+    i16 value lies within one step of zero (where the signs are decided), plus the
+    centres of random air and material bricks; the distances before quantisation of the
+    sampled bricks' nodes (icam_bricks in the same precision) against the oracle's.
+    With `decision` (the oracle's map from its decide), the bake's air and material
+    entries outside the read set are checked against it whole."""
+    rng = np.random.default_rng(seed)
+    diag = float(np.linalg.norm(np.asarray(oracle.bbox()[1]) - np.asarray(oracle.bbox()[0])))
+    stored = np.nonzero(m < 0xFFFFFFF0)[0]
+    out = {"stored_bricks": int(len(stored))}
+    # every node within one i16 step of zero, over every stored brick (chunks of the atlas)
+    near_ids, near_nodes, near_q = [], [], []
+    for c0 in range(0, len(stored), 20000):
+        ids = stored[c0:c0 + 20000]
+        q = part_gpu.unpack_atlas(a[m[ids]]).astype(np.int64)
+        bi, ni = np.nonzero(np.abs(q) <= 1)
+        near_ids.append(ids[bi])
+        near_nodes.append(ni)
+        near_q.append(q[bi, ni])
+    near_ids, near_nodes, near_q = (np.concatenate(x) if x else np.zeros(0, np.int64)
+                                    for x in (near_ids, near_nodes, near_q))
+    pick = rng.choice(stored, min(n_bricks, len(stored)), replace=False) if len(stored) else stored
+    nodes = np.arange(0, 729, every)
+    s_ids = np.repeat(pick, len(nodes))
+    s_nodes = np.tile(nodes, len(pick))
+    s_q = part_gpu.unpack_atlas(a[m[pick]]).astype(np.int64)[:, nodes].reshape(-1) if len(pick) else s_ids
+    ids = np.concatenate([near_ids, s_ids])
+    nn = np.concatenate([near_nodes, s_nodes])
+    qs = np.concatenate([near_q, s_q])
+    d = oracle.sdf(node_points(ids, nn, lo, nb, h))[0] if len(ids) else np.zeros(0)
+    qo = np.round(np.clip(d / clamp, -1.0, 1.0) * 32767.0).astype(np.int64)
+    off = np.abs(qo - qs)
+    flips = int(((qs > 0) & (qo < 0)).sum() + ((qs < 0) & (qo > 0)).sum())
+    out.update({"nodes_checked": int(len(ids)), "nodes_near_zero": int(len(near_ids)),
+                "i16_max_step_diff": int(off.max()) if len(off) else 0, "i16_nodes_off": int((off > 0).sum()),
+                "sign_flips": flips})
+    # distances before quantisation on the sampled bricks
+    if len(pick):
+        sub = pick[: min(len(pick), 256)]
+        vals, dg = g.bricks(brick_firsts(sub, lo, nb, h), h, clamp, precision=precision)
+        do = oracle.sdf(node_points(np.repeat(sub, len(nodes)), np.tile(nodes, len(sub)), lo, nb, h))[0]
+        dgs = dg[:, nodes].reshape(-1)
+        fl = vals[:, nodes, 1].reshape(-1)
+        ex = fl == 0
+        err = np.abs(dgs[ex] - do[ex])
+        out.update({"distance_max_abs_mm": float(err.max()) if len(err) else 0.0,
+                    "distance_max_over_diag": float(err.max() / diag) if len(err) else 0.0,
+                    "distance_sign_flips": int(((dgs[ex] > 0) & (do[ex] < 0)).sum() + ((dgs[ex] < 0) & (do[ex] > 0)).sum()),
+                    "flags_past_clamp_ok": bool((np.abs(do[fl == 1]) >= clamp * (1 - 1e-12)).all()),
+                    "flags_undecided": int((fl == 2).sum())})
+    # air and material bricks: the centre on the right side
+    bad = 0
+    for val in (part_gpu.AIR, part_gpu.SOLID):
+        cand = np.nonzero(m == val)[0]
+        if len(cand):
+            ids2 = rng.choice(cand, min(n_centres, len(cand)), replace=False)
+            dc = oracle.sdf(brick_firsts(ids2, lo, nb, h) + 4 * h)[0]
+            bad += int(((dc > 0) != (val == part_gpu.AIR)).sum())
+    out["air_solid_centres_wrong"] = bad
+    if decision is not None:
+        dec = decision != part_gpu.READ
+        out["decided_entries_differ"] = int((m[dec] != decision[dec]).sum())
+        out["stored_outside_read_set"] = int((m[dec] < 0xFFFFFFF0).sum())
+    out["sample"] = (f"every {every}th node of {len(pick)} random stored bricks, every node within an i16 step "
+                     f"of zero ({len(near_ids)}), {n_centres} centres of air and of material bricks; distances on "
+                     f"{min(len(pick), 256)} of the sampled bricks")
+    return out
 
 
 if __name__ == "__main__":

@@ -34,17 +34,34 @@ def sources_newer() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compiles every source to an object in parallel (one nvcc a file, the kernels
+    launched across files need no relocatable device code), then links the library."""
     if not force and not sources_newer():
         return OUT
-    cmd = [nvcc(), "-shared", "-Xcompiler", "-fPIC", "-std=c++17", "-O3", "-lineinfo", *ARCH,
-           "-o", OUT + ".tmp", *[os.path.join(CSRC, s) for s in SOURCES]]
+    from concurrent.futures import ThreadPoolExecutor
+
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    flags = ["-Xcompiler", "-fPIC", "-std=c++17", "-O3", "-lineinfo", *ARCH]
     if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-    r = subprocess.run(cmd, capture_output=True, text=True)
+        flags.insert(0, "-Xptxas=-v")
+
+    def compile_one(src):
+        obj = os.path.join(objdir, src + ".o")
+        r = subprocess.run([nvcc(), "-c", *flags, "-o", obj, os.path.join(CSRC, src)], capture_output=True, text=True)
+        return src, obj, r
+
+    with ThreadPoolExecutor(max_workers=min(len(SOURCES), os.cpu_count() or 1)) as ex:
+        results = list(ex.map(compile_one, SOURCES))
+    for src, _, r in results:
+        if r.returncode != 0:
+            raise RuntimeError(f"nvcc failed on {src}:\n" + r.stdout + r.stderr)
+        if verbose:
+            sys.stderr.write(r.stderr)
+    r = subprocess.run([nvcc(), "-shared", *ARCH, "-o", OUT + ".tmp", *[o for _, o, _ in results]],
+                       capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
-    if verbose:
-        sys.stderr.write(r.stderr)
+        raise RuntimeError("nvcc link failed:\n" + r.stdout + r.stderr)
     os.replace(OUT + ".tmp", OUT)
     return OUT
 

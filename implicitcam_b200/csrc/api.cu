@@ -201,6 +201,10 @@ int icam_points(IcamPack* pk, const double* xyz, size_t n, double clamp, int cap
                 double* value_out, int8_t* flag_out) {
   if (!pk || (!xyz && n) || (!value_out && n) || (!flag_out && n)) return fail(pk, ICAM_ERR_ARG, "null argument");
   if (precision < ICAM_FP64 || precision > ICAM_MIXED_LEARNED) return fail(pk, ICAM_ERR_ARG, "unknown precision");
+  // Scattered points share no centre, so the mixed forms' float solves (seeded and
+  // rebased per brick) have nothing to stand on: points are read in double precision only.
+  if (precision != ICAM_FP64)
+    return fail(pk, ICAM_ERR_ARG, "icam_points reads in ICAM_FP64 only (the mixed forms are brick reads)");
   if (n == 0) return ICAM_OK;
   CK(cudaSetDevice(pk->device));
   void *dx, *dv, *df;
@@ -327,6 +331,8 @@ int decide_level(IcamPack* pk, const LevelDesc& L, DecideOut* out) {
   void* d_first;
   if ((r = scratch(pk, 16, first.size() * (sizeof(double) + 1) + 16, &d_first))) return r;
   CK(cudaMemcpyAsync(d_cur, first.data(), first.size() * sizeof(Box4), cudaMemcpyHostToDevice, s));
+  out->h2d_bytes = int64_t(first.size() * sizeof(Box4));
+  out->d2h_bytes = 0;
   int64_t ncur = int64_t(first.size()), boxes_read = 0;
   unsigned long long* cnt = (unsigned long long*)d_cnt;
   while (ncur > 0) {
@@ -361,6 +367,7 @@ int decide_level(IcamPack* pk, const LevelDesc& L, DecideOut* out) {
     unsigned long long nn = 0;
     CK(cudaMemcpyAsync(&nn, cnt, sizeof(nn), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    out->d2h_bytes += sizeof(nn);
     boxes_read += ncur;
     if (int64_t(nn) > box_cap) return fail(pk, ICAM_ERR_ROOM, "box list overflow");
     std::swap(d_cur, d_next);
@@ -370,6 +377,7 @@ int decide_level(IcamPack* pk, const LevelDesc& L, DecideOut* out) {
   unsigned long long nread = 0;
   CK(cudaMemcpyAsync(&nread, cnt + 1, sizeof(nread), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
+  out->d2h_bytes += sizeof(nread);
   const int64_t R = int64_t(nread);
   // the read bricks in brick order (partcache.rs:486)
   void *d_ridx2, *d_rdc2, *d_tmp;
@@ -404,10 +412,13 @@ static int bake_level(IcamPack* pk, double h, const double lo[3], const int64_t 
   if (precision < ICAM_FP64 || precision > ICAM_MIXED_LEARNED) return fail(pk, ICAM_ERR_ARG, "unknown precision");
   CK(cudaSetDevice(pk->device));
   cudaStream_t s = pk->stream;
+  pk->last_map = pk->last_atlas = nullptr;  // the scratch they live in is about to change
+  pk->last_map_entries = pk->last_slots = 0;
   LevelDesc L;
   L.h = h, L.clamp = clamp;
   for (int k = 0; k < 3; k++) L.lo[k] = lo[k], L.nb[k] = nb[k], L.origin[k] = origin ? origin[k] : 0.0;
   L.has_origin = origin != nullptr;
+  L.precision = precision;
   cudaEvent_t ev[5];
   for (auto& e : ev) CK(cudaEventCreate(&e));
   CK(cudaEventRecord(ev[0], s));
@@ -465,8 +476,9 @@ static int bake_level(IcamPack* pk, double h, const double lo[3], const int64_t 
     int64_t ns = 0;
     CK(cudaMemcpyAsync(&ns, (int64_t*)d_slot + R, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    D.d2h_bytes += sizeof(ns);
     nwords_slots = size_t(ns);
-    if ((r = scratch(pk, 2, std::max<size_t>(nwords_slots, 1) * 365 * sizeof(uint32_t), &d_atlas))) return r;
+    if ((r = scratch(pk, 17, std::max<size_t>(nwords_slots, 1) * 365 * sizeof(uint32_t), &d_atlas))) return r;
     k_assemble<<<grid_for(R, 1), 128, 0, s>>>((const int64_t*)d_ridx2, (const int32_t*)d_kind, (const int64_t*)d_slot,
                                               R, (const uint32_t*)d_words, (uint32_t*)d_map, (uint32_t*)d_atlas);
     launches += 3;
@@ -474,13 +486,17 @@ static int bake_level(IcamPack* pk, double h, const double lo[3], const int64_t 
   } else {
     CK(cudaEventRecord(ev[2], s));
     CK(cudaEventRecord(ev[3], s));
-    if ((r = scratch(pk, 2, 365 * sizeof(uint32_t), &d_atlas))) return r;
+    if ((r = scratch(pk, 17, 365 * sizeof(uint32_t), &d_atlas))) return r;
   }
   CK(cudaEventRecord(ev[4], s));
   CK(cudaStreamSynchronize(s));
   *n_slots = nwords_slots;
   *d_map_out = (const uint32_t*)d_map;
   *d_atlas_out = (const uint32_t*)d_atlas;
+  pk->last_map = (const uint32_t*)d_map;
+  pk->last_atlas = (const uint32_t*)d_atlas;
+  pk->last_map_entries = size_t(nb[0] * nb[1] * nb[2]);
+  pk->last_slots = nwords_slots;
   if (stats) {
     unsigned long long st[16] = {0};
     CK(cudaMemcpy(st, pk->d_stats, sizeof(st), cudaMemcpyDeviceToHost));
@@ -495,6 +511,8 @@ static int bake_level(IcamPack* pk, double h, const double lo[3], const int64_t 
     for (int k = 0; k < 5; k++) stats->census[k] = R ? int64_t(st[6 + k]) : 0;
     stats->bricks_settled = R ? int64_t(st[11]) : 0;
     stats->kernel_launches = launches;
+    stats->h2d_bytes = D.h2d_bytes;
+    stats->d2h_bytes = D.d2h_bytes + int64_t(sizeof(st));
     float ms;
     cudaEventElapsedTime(&ms, ev[0], ev[1]);
     stats->ms_decide = ms;
@@ -514,11 +532,79 @@ int icam_bake_level(IcamPack* pk, double h, const double lo[3], const int64_t nb
   int rc = bake_level(pk, h, lo, nb, clamp, origin, precision, n_slots, stats, &dm, &da);
   if (rc) return rc;
   int64_t total = nb[0] * nb[1] * nb[2];
-  if (map_out) CK(cudaMemcpyAsync(map_out, dm, total * sizeof(uint32_t), cudaMemcpyDeviceToHost, pk->stream));
+  if (map_out) {
+    CK(cudaMemcpyAsync(map_out, dm, total * sizeof(uint32_t), cudaMemcpyDeviceToHost, pk->stream));
+    if (stats) stats->d2h_bytes += total * int64_t(sizeof(uint32_t));
+  }
   if (atlas_out) {
     if (*n_slots * 365 > atlas_cap_words) return fail(pk, ICAM_ERR_ARG, "atlas_out too small");
     CK(cudaMemcpyAsync(atlas_out, da, *n_slots * 365 * sizeof(uint32_t), cudaMemcpyDeviceToHost, pk->stream));
+    if (stats) stats->d2h_bytes += int64_t(*n_slots * 365 * sizeof(uint32_t));
   }
+  CK(cudaStreamSynchronize(pk->stream));
+  return ICAM_OK;
+}
+
+int icam_decide_level(IcamPack* pk, double h, const double lo[3], const int64_t nb[3], double clamp,
+                      const double origin[3], int precision, uint32_t* map_out, int64_t* read_out, double* dc_out,
+                      size_t read_cap, size_t* n_read, IcamBakeStats* stats) {
+  if (!pk || !lo || !nb || !n_read) return fail(pk, ICAM_ERR_ARG, "null argument");
+  if (precision < ICAM_FP64 || precision > ICAM_MIXED_LEARNED) return fail(pk, ICAM_ERR_ARG, "unknown precision");
+  CK(cudaSetDevice(pk->device));
+  cudaStream_t s = pk->stream;
+  pk->last_map = pk->last_atlas = nullptr;  // the decision reuses the bake's scratch
+  pk->last_map_entries = pk->last_slots = 0;
+  LevelDesc L;
+  L.h = h, L.clamp = clamp;
+  for (int k = 0; k < 3; k++) L.lo[k] = lo[k], L.nb[k] = nb[k], L.origin[k] = origin ? origin[k] : 0.0;
+  L.has_origin = origin != nullptr;
+  L.precision = precision;
+  cudaEvent_t ev[2];
+  for (auto& e : ev) CK(cudaEventCreate(&e));
+  CK(cudaEventRecord(ev[0], s));
+  DecideOut D;
+  int r = decide_level(pk, L, &D);
+  if (r) {
+    for (auto& e : ev) cudaEventDestroy(e);
+    return r;
+  }
+  CK(cudaEventRecord(ev[1], s));
+  *n_read = size_t(D.n_read);
+  const int64_t total = nb[0] * nb[1] * nb[2];
+  if (map_out) CK(cudaMemcpyAsync(map_out, D.map, total * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  const size_t m = std::min(size_t(D.n_read), read_cap);
+  if (read_out && m) CK(cudaMemcpyAsync(read_out, D.read_idx, m * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  if (dc_out && m) CK(cudaMemcpyAsync(dc_out, D.read_dc, m * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->boxes_read = D.boxes_read;
+    stats->bricks_read = D.n_read;
+    stats->kernel_launches = D.launches;
+    float ms;
+    cudaEventElapsedTime(&ms, ev[0], ev[1]);
+    stats->ms_decide = ms;
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  if ((read_out || dc_out) && size_t(D.n_read) > read_cap)
+    return fail(pk, ICAM_ERR_ARG, "icam_decide_level: read_cap is below the bricks to read (*n_read)");
+  return ICAM_OK;
+}
+
+int icam_level_read(IcamPack* pk, uint32_t* map_out, size_t map_entries, uint32_t* atlas_out,
+                    size_t atlas_cap_words) {
+  if (!pk) return ICAM_ERR_ARG;
+  if (!pk->last_map) return fail(pk, ICAM_ERR_ARG, "icam_level_read: no level baked on this pack");
+  if (map_out && map_entries != pk->last_map_entries)
+    return fail(pk, ICAM_ERR_ARG, "icam_level_read: map_entries is not the level's brick count");
+  if (atlas_out && atlas_cap_words < pk->last_slots * 365)
+    return fail(pk, ICAM_ERR_ARG, "icam_level_read: atlas_out holds fewer than n_slots x 365 words");
+  CK(cudaSetDevice(pk->device));
+  if (map_out)
+    CK(cudaMemcpyAsync(map_out, pk->last_map, map_entries * sizeof(uint32_t), cudaMemcpyDeviceToHost, pk->stream));
+  if (atlas_out && pk->last_slots)
+    CK(cudaMemcpyAsync(atlas_out, pk->last_atlas, pk->last_slots * 365 * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                       pk->stream));
   CK(cudaStreamSynchronize(pk->stream));
   return ICAM_OK;
 }
@@ -642,7 +728,9 @@ int icam_warm(IcamPack* pk, double secs) {
 // must start at zero; each call clears them on the pack's stream before the kernel.
 // The first call on a device looks the array's address up (cudaGetSymbolAddress,
 // with that device current), which may load this library's device code; make that
-// first call before any stream capture.
+// first call before any stream capture. The address is kept for the life of the
+// process: after a cudaDeviceReset of that device (which unloads the array) it is
+// stale, so no call may follow a reset.
 // ---------------------------------------------------------------------------
 
 namespace {
@@ -694,6 +782,10 @@ extern "C" int icam_bricks_static(IcamPack* pk, const double* first_nodes, size_
   }
   if (pk->device < 0 || pk->device >= kStaticDevices)
     return static_fail(err, errlen, ICAM_ERR_ARG, "device ordinal out of range", nullptr);
+  // ICAM_MIXED_LEARNED needs the pack's trained seed network, as icam_bricks does
+  if (precision == ICAM_MIXED_LEARNED && !pk->net.ready)
+    return static_fail(err, errlen, ICAM_ERR_ARG,
+                       "ICAM_MIXED_LEARNED: train (icam_seednet_train) or load the seed network first", nullptr);
   if (n == 0) return ICAM_OK;
   SCK(cudaSetDevice(pk->device));
   unsigned char* base = static_cast<unsigned char*>(g_static_addr[pk->device].load(std::memory_order_acquire));
@@ -721,6 +813,10 @@ extern "C" int icam_bricks_static(IcamPack* pk, const double* first_nodes, size_
   a.leaves = pk->leaves;
   a.n_leaves = int32_t(pk->leaves_host.size());
   a.mixed = precision != ICAM_FP64;
+  if (precision == ICAM_MIXED_LEARNED) {  // the starts the seed network puts, as icam_bricks takes them
+    a.net_feat = pk->net.feat;
+    a.net_w = pk->net.wbf;
+  }
   a.d_out = dval;
   a.flag_out = dflag;
   a.stats = stats;

@@ -36,6 +36,7 @@ struct LevelDesc {
   double lo[3] = {0, 0, 0}, origin[3] = {0, 0, 0};
   int64_t nb[3] = {0, 0, 0};
   bool has_origin = false;
+  int precision = 0;  // ICAM_FP64, ICAM_MIXED or ICAM_MIXED_LEARNED
 };
 
 // The box decision of a level, left on the device in the pack's scratch: the map (read
@@ -45,6 +46,7 @@ struct DecideOut {
   int64_t* read_idx = nullptr;
   double* read_dc = nullptr;
   int64_t n_read = 0, boxes_read = 0, launches = 0;
+  int64_t h2d_bytes = 0, d2h_bytes = 0;  // host copies the decision made
 };
 
 namespace icam {
@@ -70,10 +72,12 @@ struct IcamPack {
     void* p = nullptr;
     size_t n = 0;
   };
-  Buf scratch[17];
+  Buf scratch[24];
   std::string err;
   unsigned long long* d_stats = nullptr;
+  // the last level bake's results (scratch 3 and 17), for icam_level_read
   const uint32_t* last_map = nullptr;
   const uint32_t* last_atlas = nullptr;
+  size_t last_map_entries = 0, last_slots = 0;
   SeedNetState net;
 };

@@ -19,6 +19,7 @@ LIB = os.path.join(HERE, "libicam_cuda.so")
 
 FP64, MIXED, MIXED_LEARNED = 0, 1, 2
 AIR, SOLID, WORDS = 0xFFFFFFFF, 0xFFFFFFFE, 365
+READ = 0xFFFFFFF0  # a brick the box decision leaves to be read
 
 _lib = None
 
@@ -33,7 +34,7 @@ class IcamBakeStats(C.Structure):
         ("nodes_exact", C.c_int64), ("nodes_far", C.c_int64), ("nodes_undecided", C.c_int64),
         ("pairs", C.c_int64), ("fallback_nodes", C.c_int64), ("kernel_launches", C.c_int64),
         ("ms_decide", C.c_double), ("ms_cull", C.c_double), ("ms_nodes", C.c_double), ("ms_post", C.c_double),
-        ("census", C.c_int64 * 5), ("bricks_settled", C.c_int64),
+        ("census", C.c_int64 * 5), ("bricks_settled", C.c_int64), ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64),
     ]
 
     def as_dict(self):
@@ -82,6 +83,9 @@ def lib():
         L.icam_points.argtypes = [vp, vp, sz, C.c_double, C.c_int, C.c_int, vp, vp]
         L.icam_bricks.argtypes = [vp, vp, sz, C.c_double, C.c_double, C.c_int, vp, vp]
         L.icam_bake_level.argtypes = [vp, C.c_double, vp, vp, C.c_double, vp, C.c_int, vp, vp, sz, C.POINTER(sz), vp]
+        L.icam_level_read.argtypes = [vp, vp, sz, vp, sz]
+        L.icam_decide_level.argtypes = [vp, C.c_double, vp, vp, C.c_double, vp, C.c_int, vp, vp, vp, sz,
+                                        C.POINTER(sz), vp]
         L.icam_bake_level_device.argtypes = [vp, C.c_double, vp, vp, C.c_double, vp, C.c_int, C.POINTER(vp),
                                              C.POINTER(vp), C.POINTER(sz), vp]
         L.icam_list.argtypes = [vp, vp, C.c_double, C.c_double, vp, sz, C.POINTER(sz)]
@@ -185,15 +189,39 @@ class PartGpu:
         m = np.zeros(int(np.prod(nb)), np.uint32)
         ns = C.c_size_t()
         st = IcamBakeStats()
-        # first the slot count, then the atlas sized to it
+        # one bake for the map and the slot count, then the atlas sized to it read back
         self._check(lib().icam_bake_level(self.h, float(h), _p(lo), _p(nb), float(clamp), _p(org), precision, _p(m),
                                           None, 0, C.byref(ns), C.byref(st)), "icam_bake_level")
         if not atlas:
             return m, None, st.as_dict()
         a = np.zeros((ns.value, WORDS), np.uint32)
-        self._check(lib().icam_bake_level(self.h, float(h), _p(lo), _p(nb), float(clamp), _p(org), precision, _p(m),
-                                          _p(a), a.size, C.byref(ns), C.byref(st)), "icam_bake_level")
+        self._check(lib().icam_level_read(self.h, None, 0, _p(a), a.size), "icam_level_read")
         return m, a, st.as_dict()
+
+    def decide(self, h, lo, nb, clamp=None, origin=None, precision=FP64):
+        """The level's box decision alone (PartCache::decide, partcache.rs:226-331):
+        (map with READ at the bricks to read, their indices in brick order, their
+        centres' distances, stats)."""
+        lo = np.ascontiguousarray(lo, dtype=np.float64)
+        nb = np.ascontiguousarray(nb, dtype=np.int64)
+        clamp = h * np.sqrt(3.0) if clamp is None else clamp
+        org = None if origin is None else np.ascontiguousarray(origin, dtype=np.float64)
+        total = int(np.prod(nb))
+        m = np.zeros(total, np.uint32)
+        idx = np.zeros(total, np.int64)
+        dc = np.zeros(total)
+        n = C.c_size_t()
+        st = IcamBakeStats()
+        self._check(lib().icam_decide_level(self.h, float(h), _p(lo), _p(nb), float(clamp), _p(org), precision, _p(m),
+                                            _p(idx), _p(dc), total, C.byref(n), C.byref(st)), "icam_decide_level")
+        return m, idx[: n.value].copy(), dc[: n.value].copy(), st.as_dict()
+
+    def level_read(self, map_entries, slots):
+        """The last level baked on this pack, read back without baking again: (map, atlas)."""
+        m = np.zeros(int(map_entries), np.uint32)
+        a = np.zeros((int(slots), WORDS), np.uint32)
+        self._check(lib().icam_level_read(self.h, _p(m), m.size, _p(a), a.size), "icam_level_read")
+        return m, a
 
     def level_into(self, h, lo, nb, clamp, map_out, atlas_out, origin=None, precision=FP64):
         """The bake with its map and atlas written into caller buffers (numpy arrays or

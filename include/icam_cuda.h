@@ -34,6 +34,7 @@ extern "C" {
 #define ICAM_AIR 0xffffffffu   /* cache.rs:84 AIR */
 #define ICAM_SOLID 0xfffffffeu /* cache.rs:85 SOLID */
 #define ICAM_WORDS 365         /* cache.rs:91 WORDS */
+#define ICAM_READ 0xfffffff0u  /* a brick the box decision leaves to be read (icam_decide_level) */
 #define ICAM_NODES 729
 
 /* Arithmetic of the per-node evaluation. */
@@ -80,6 +81,9 @@ typedef struct IcamBakeStats {
    * step, known from the brick's centre distance (the field is 1-Lipschitz): air or
    * solid without reading their nodes. */
   int64_t bricks_settled;
+  /* Bytes the call copied from host to device (the decision's first boxes) and from
+   * device to host (its counts, and for icam_bake_level the map and atlas). */
+  int64_t h2d_bytes, d2h_bytes;
 } IcamBakeStats;
 
 /* Packs the solid for the device (PartGpu::new, partgpu.rs:132; Exact::gpu_pack,
@@ -98,7 +102,9 @@ int icam_pack_info(const IcamPack* pack, int64_t counts[7]);
  * capped != 0 a point needs an exact value only within `clamp` (past it the
  * answer may be the bound, flag 1), as PartGpu::points_scatter_capped
  * (partgpu.rs:249); with capped == 0 every point is read exactly
- * (PartGpu::points_refined, partgpu.rs:243). Host arrays. */
+ * (PartGpu::points_refined, partgpu.rs:243). Host arrays. Points are read in double
+ * precision: `precision` must be ICAM_FP64 (the mixed forms, which rebase and seed
+ * their float solves per brick, are brick reads), else ICAM_ERR_ARG. */
 int icam_points(IcamPack* pack, const double* xyz, size_t n, double clamp, int capped, int precision,
                 double* value_out, int8_t* flag_out);
 
@@ -116,10 +122,13 @@ int icam_bricks(IcamPack* pack, const double* first_nodes, size_t n, double h, d
  * wait of cudaFree). Same kernel and outputs as icam_bricks, with every buffer in
  * one fixed device array of the library (one per device, about 3 MB) that all
  * calls on that device share: calls that overlap in time race on it. n above
- * ICAM_STATIC_BRICKS is refused with ICAM_ERR_ROOM. The first call on a device
- * resolves the array's address and may load the library's device code: make it
- * before any stream capture. Errors are written to err (errlen bytes), not to the
- * pack's message. */
+ * ICAM_STATIC_BRICKS is refused with ICAM_ERR_ROOM; ICAM_MIXED_LEARNED on a pack
+ * whose seed network is neither trained nor loaded with ICAM_ERR_ARG, as icam_bricks
+ * refuses it. The call returns once the results are in values_out / d_out. The first
+ * call on a device resolves the array's address and may load the library's device
+ * code: make it before any stream capture. The address is kept until the process
+ * exits, so no call may follow a cudaDeviceReset of that device. Errors are written
+ * to err (errlen bytes), not to the pack's message. */
 #define ICAM_STATIC_BRICKS 256
 int icam_bricks_static(IcamPack* pack, const double* first_nodes, size_t n, double h, double clamp, int precision,
                        float* values_out, double* d_out, char* err, size_t errlen);
@@ -132,15 +141,38 @@ int icam_bricks_static(IcamPack* pack, const double* first_nodes, size_t n, doub
  * bridges the undecided ones, quantises and packs them (partcache.rs:759-970).
  * map_out: nb[0]*nb[1]*nb[2] entries, x fastest (slot, ICAM_AIR or ICAM_SOLID);
  * atlas_out: up to atlas_cap_words words, slots of 365 words in brick order;
- * *n_slots: the slots written. A NULL atlas_out returns *n_slots only. */
+ * *n_slots: the slots written. A NULL atlas_out returns *n_slots only, and an atlas_out
+ * too small for them ICAM_ERR_ARG; either way the level stays on the device for
+ * icam_level_read, so sizing the atlas needs no second bake. */
 int icam_bake_level(IcamPack* pack, double h, const double lo[3], const int64_t nb[3], double clamp,
                     const double origin[3], int precision, uint32_t* map_out, uint32_t* atlas_out,
                     size_t atlas_cap_words, size_t* n_slots, IcamBakeStats* stats);
 
+/* The box decision of a level alone (PartCache::decide, partcache.rs:226-331), with the
+ * arguments of icam_bake_level: map_out (nb[0]*nb[1]*nb[2] entries, x fastest) holds
+ * ICAM_AIR / ICAM_SOLID for the bricks decided and ICAM_READ for the bricks to read;
+ * read_out / dc_out (optional, read_cap entries) the bricks to read in brick order
+ * (partcache.rs:486) and their centres' signed distances (NaN where the decision does
+ * not need one); *n_read their count (ICAM_ERR_ARG when above read_cap with an output
+ * given). stats: boxes_read, bricks_read, kernel_launches, ms_decide. The mixed forms
+ * decide the same bricks as ICAM_FP64. */
+int icam_decide_level(IcamPack* pack, double h, const double lo[3], const int64_t nb[3], double clamp,
+                      const double origin[3], int precision, uint32_t* map_out, int64_t* read_out, double* dc_out,
+                      size_t read_cap, size_t* n_read, IcamBakeStats* stats);
+
+/* The last level baked on the pack (by icam_bake_level or icam_bake_level_device),
+ * copied to host arrays without baking again: map_out (map_entries = the level's
+ * nb[0]*nb[1]*nb[2] entries) and atlas_out (atlas_cap_words >= n_slots x 365), either
+ * may be NULL. The sizing pattern is one bake with atlas_out NULL for *n_slots, then
+ * this read into an atlas of that size. No counterpart in the reference, whose level
+ * bake returns owned vectors. ICAM_ERR_ARG when no level was baked or a size is wrong. */
+int icam_level_read(IcamPack* pack, uint32_t* map_out, size_t map_entries, uint32_t* atlas_out,
+                    size_t atlas_cap_words);
+
 /* The same bake, its results left in device memory the pack owns (valid until the
- * next bake on the pack): *d_map and *d_atlas are device pointers. For callers
- * that consume the level on the GPU (the reference's viewer uploads it to its ray
- * caster). */
+ * next bake on the pack; the pack's point and brick reads do not touch them):
+ * *d_map and *d_atlas are device pointers. For callers that consume the level on the
+ * GPU (the reference's viewer uploads it to its ray caster). */
 int icam_bake_level_device(IcamPack* pack, double h, const double lo[3], const int64_t nb[3], double clamp,
                            const double origin[3], int precision, const uint32_t** d_map,
                            const uint32_t** d_atlas, size_t* n_slots, IcamBakeStats* stats);

@@ -60,7 +60,7 @@ def test_no_gpu_fails_loudly():
 
 
 def test_rust_binding_names_match_the_header():
-    """INTEGRATION.md's extern block binds exactly the header's entry points."""
+    """The Rust extern block of the integration guide binds exactly the header's entry points."""
     text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
     rust = sorted(set(re.findall(r"pub fn (icam_\w+)\(", text)))
     assert rust == declared()
