@@ -375,6 +375,7 @@ def main():
             "bricks_read": st["bricks_read"], "bricks_stored": st["bricks_words"],
             "bricks_settled": st["bricks_settled"],
             "nodes_exact": st["nodes_exact"], "nodes_undecided": st["nodes_undecided"],
+            "nodes_double": st["nodes_double"], "centres_double": st["centres_double"],
             "nodes_exact_per_s": st["nodes_exact"] * args.steps / (total_ms * 1e-3),
             "stage_ms": {"decide": st["ms_decide"], "nodes": st["ms_nodes"], "assemble": st["ms_post"]},
             "gpu_launches": int(st["kernel_launches"]) * args.steps,
@@ -634,9 +635,10 @@ def verify_against_oracle(g, oracle, part_gpu, lo, nb, h, clamp, precision, m, a
         fl = vals[:, nodes, 1].reshape(-1)
         ex = fl == 0
         err = np.abs(dgs[ex] - do[ex])
+        sg = ex & (np.abs(do) > 1e-9)  # signs above double rounding
         out.update({"distance_max_abs_mm": float(err.max()) if len(err) else 0.0,
                     "distance_max_over_diag": float(err.max() / diag) if len(err) else 0.0,
-                    "distance_sign_flips": int(((dgs[ex] > 0) & (do[ex] < 0)).sum() + ((dgs[ex] < 0) & (do[ex] > 0)).sum()),
+                    "distance_sign_flips": int(((dgs[sg] > 0) & (do[sg] < 0)).sum() + ((dgs[sg] < 0) & (do[sg] > 0)).sum()),
                     "flags_past_clamp_ok": bool((np.abs(do[fl == 1]) >= clamp * (1 - 1e-12)).all()),
                     "flags_undecided": int((fl == 2).sum())})
     # air and material bricks: the centre on the right side

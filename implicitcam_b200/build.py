@@ -12,7 +12,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libicam_cuda.so")
-SOURCES = ["api.cu", "kernels.cu", "bricks.cu", "decide.cu", "seednet.cu", "batch.cu", "pack_build.cpp", "host_geom.cpp"]
+SOURCES = ["api.cu", "kernels.cu", "bricks.cu", "bricks_mixed.cu", "decide.cu", "seednet.cu", "batch.cu", "pack_build.cpp", "host_geom.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

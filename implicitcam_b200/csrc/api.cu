@@ -355,13 +355,14 @@ int decide_level(IcamPack* pk, const LevelDesc& L, DecideOut* out) {
     a.read_cap = total;
     a.n_read = cnt + 1;
     const bool is_first = launches == 0;
+    a.n_double = cnt + 2;
     if (is_first) {
       a.first_sd = static_cast<double*>(d_first);
       a.first_sign = reinterpret_cast<int8_t*>(static_cast<double*>(d_first) + ncur);
       for (int k = 0; k < 3; k++) a.first_dims[k] = dims[k];
     }
     CK(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), s));
-    launch_decide(a, s, is_first);
+    launch_decide(a, s, is_first, L.precision != ICAM_FP64);
     launches += is_first ? 2 : 1;
     CK(cudaGetLastError());
     unsigned long long nn = 0;
@@ -375,9 +376,12 @@ int decide_level(IcamPack* pk, const LevelDesc& L, DecideOut* out) {
     size /= 2;
   }
   unsigned long long nread = 0;
-  CK(cudaMemcpyAsync(&nread, cnt + 1, sizeof(nread), cudaMemcpyDeviceToHost, s));
+  unsigned long long cnt_host[4] = {0, 0, 0, 0};
+  CK(cudaMemcpyAsync(cnt_host, cnt, sizeof(cnt_host), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
-  out->d2h_bytes += sizeof(nread);
+  out->d2h_bytes += sizeof(cnt_host);
+  nread = cnt_host[1];
+  out->centres_double = int64_t(cnt_host[2]);
   const int64_t R = int64_t(nread);
   // the read bricks in brick order (partcache.rs:486)
   void *d_ridx2, *d_rdc2, *d_tmp;
@@ -511,6 +515,8 @@ static int bake_level(IcamPack* pk, double h, const double lo[3], const int64_t 
     for (int k = 0; k < 5; k++) stats->census[k] = R ? int64_t(st[6 + k]) : 0;
     stats->bricks_settled = R ? int64_t(st[11]) : 0;
     stats->kernel_launches = launches;
+    stats->nodes_double = R ? int64_t(st[12]) : 0;
+    stats->centres_double = D.centres_double;
     stats->h2d_bytes = D.h2d_bytes;
     stats->d2h_bytes = D.d2h_bytes + int64_t(sizeof(st));
     float ms;
@@ -581,6 +587,9 @@ int icam_decide_level(IcamPack* pk, double h, const double lo[3], const int64_t 
     stats->boxes_read = D.boxes_read;
     stats->bricks_read = D.n_read;
     stats->kernel_launches = D.launches;
+    stats->centres_double = D.centres_double;
+    stats->h2d_bytes = D.h2d_bytes;
+    stats->d2h_bytes = D.d2h_bytes;
     float ms;
     cudaEventElapsedTime(&ms, ev[0], ev[1]);
     stats->ms_decide = ms;

@@ -312,6 +312,7 @@ int icam_batch_bake(IcamBatch* bt, const IcamBatchLevel* levels, int precision, 
   BCK(cudaMemcpyAsync(d_args, args.data(), args.size() * sizeof(DecideArgs), cudaMemcpyHostToDevice, s));
   BCK(cudaMemcpyAsync(d_roff, lvl_off.data(), (n + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
   DecideBatchArgs db{};
+  db.mixed = precision != ICAM_FP64;
   db.args = static_cast<const DecideArgs*>(d_args);
   db.n_parts = n;
   db.cnt = c;

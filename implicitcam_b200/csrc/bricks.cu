@@ -5,23 +5,12 @@
 
 #include "kernels.h"
 #include "seednet.cuh"
+#include "brick_post.cuh"
 #include "warp_list.cuh"
 
 namespace icam {
 
 constexpr int MAX_WARPS = 4;  // bricks a block works on at once, one a warp (1, 2 or 4)
-
-// The 26 neighbours of node n inside the brick, in the reference's order (dk, dj, di
-// from -1 to 1, partcache.rs:829-839).
-__device__ __forceinline__ int nb_of(int n, int k, double* dist) {
-  int i = n % 9, j = (n / 9) % 9, kk = n / 81;
-  int o = k < 13 ? k : k + 1;  // skip (0,0,0)
-  int di = o % 3 - 1, dj = (o / 3) % 3 - 1, dk = o / 9 - 1;
-  int a = i + di, b = j + dj, c = kk + dk;
-  if (a < 0 || a > 8 || b < 0 || b > 8 || c < 0 || c > 8) return -1;
-  *dist = sqrt(double(di * di + dj * dj + dk * dk));
-  return a + 9 * b + 81 * c;
-}
 
 // A warp's shared memory for its brick. The list before its ranking and the walk's
 // frontier share room with the node values, which come later.
@@ -40,10 +29,7 @@ struct BrickSmem {
   float4 net32[16];
   union {
     Seed seed[MAXSUB];
-    // after the nodes: node masks by row (row j + 9 k, bit i of node i + 9 j + 81 k)
-    struct {
-      uint32_t m0[81], m1[81], m2[81];
-    } mk;
+    RowMasks mk;  // after the nodes: node masks by row
   } v;
   int8_t flag[729];
   int8_t cert[MAXC];
@@ -52,64 +38,6 @@ struct BrickSmem {
 };
 static_assert(sizeof(BrickSmem) * MAX_WARPS <= 48 * 1024, "shared memory of a block");
 static_assert(sizeof(((BrickSmem*)0)->u) >= 32 * SN_KS * 2 + 32 * 8 * 4, "the seed network's room in the list's");
-
-__device__ __forceinline__ uint32_t spread(uint32_t m) { return m | (m << 1) | (m >> 1); }
-
-// Row masks grown by one node in every direction (the 26-neighbourhood and the node):
-// rows r of this lane, up to three.
-__device__ __forceinline__ uint32_t dilate_row(const uint32_t* m, int r) {
-  int j = r % 9, k = r / 9;
-  uint32_t d = 0;
-#pragma unroll
-  for (int dk = -1; dk <= 1; dk++) {
-    int kk = k + dk;
-    if (kk < 0 || kk > 8) continue;
-#pragma unroll
-    for (int dj = -1; dj <= 1; dj++) {
-      int jj = j + dj;
-      if (jj < 0 || jj > 8) continue;
-      d |= spread(m[jj + 9 * kk]);
-    }
-  }
-  return d & 0x1ffu;
-}
-
-// Far nodes signed by a signed neighbour, until nothing changes (partcache.rs:845-858):
-// m0 / m1 the nodes of positive / negative value, m2 the far nodes not yet signed. A
-// far node lies farther than the clamp from the surface, so its neighbours within a
-// cell diagonal all share its sign when the clamp is at least that diagonal; a node
-// offered both signs takes the positive one.
-__device__ void flood(BrickSmem& S, int lane) {
-  for (;;) {
-    uint32_t np[3], nq[3];
-    bool any = false;
-#pragma unroll
-    for (int q = 0; q < 3; q++) {
-      int r = lane + 32 * q;
-      np[q] = nq[q] = 0;
-      if (r < 81) {
-        uint32_t o = S.v.mk.m2[r];
-        if (o) {
-          np[q] = dilate_row(S.v.mk.m0, r) & o;
-          nq[q] = dilate_row(S.v.mk.m1, r) & o & ~np[q];
-          any |= (np[q] | nq[q]) != 0;
-        }
-      }
-    }
-    __syncwarp();
-#pragma unroll
-    for (int q = 0; q < 3; q++) {
-      int r = lane + 32 * q;
-      if (r < 81 && (np[q] | nq[q])) {
-        S.v.mk.m0[r] |= np[q];
-        S.v.mk.m1[r] |= nq[q];
-        S.v.mk.m2[r] &= ~(np[q] | nq[q]);
-      }
-    }
-    __syncwarp();
-    if (!__any_sync(FULL, any)) break;
-  }
-}
 
 // One brick a warp:
 //  0. a brick whose centre distance puts every node past the clamp is written at once;
@@ -295,164 +223,11 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 2) k_bricks_t(BrickArgs a) {
     const int n_exact = __reduce_add_sync(FULL, cnt[0]), n_far = __reduce_add_sync(FULL, cnt[1]),
               n_und = __reduce_add_sync(FULL, cnt[2]);
     int provisional = 0;
-    if (a.words_out || a.kind_out) {
-      // every node far with the centre's sign known: the last rule decides them all
-      // (partcache.rs:876-892), whatever the fill and the ball would have given
-      const bool all_far = n_far == 729 && isfinite(dc) && dc != 0.0;
-      if (all_far) {
-        for (int nn = lane; nn < 729; nn += 32) S.u.f[nn] = copysign(clamp, dc);
-      } else {
-        // ---- far nodes signed by a neighbour within a cell diagonal (partcache.rs:845-858)
-        for (int r = lane; r < 81; r += 32) {
-          uint32_t pm = 0, qm = 0, om = 0;
-          for (int i = 0; i < 9; i++) {
-            double v = S.u.f[9 * r + i];
-            if (v > 0.0)
-              pm |= 1u << i;
-            else if (v < 0.0)
-              qm |= 1u << i;
-            else if (isnan(v) && S.flag[9 * r + i] == 1)
-              om |= 1u << i;
-          }
-          S.v.mk.m0[r] = pm, S.v.mk.m1[r] = qm, S.v.mk.m2[r] = om;
-        }
-        __syncwarp();
-        flood(S, lane);
-        // ---- far nodes in the centre's empty ball, or the centre in theirs (partcache.rs:860-875)
-        if (isfinite(dc) && dc != 0.0) {
-          double rch = 0.999 * fmax(clamp, fabs(dc));
-          for (int r = lane; r < 81; r += 32) {
-            uint32_t om = S.v.mk.m2[r], hit = 0;
-            for (int i = 0; i < 9; i++) {
-              if (!((om >> i) & 1u)) continue;
-              int nn = 9 * r + i;
-              double3 x = first + mk(h * (nn % 9), h * ((nn / 9) % 9), h * (nn / 81));
-              if (len(x - c) < rch) hit |= 1u << i;
-            }
-            if (hit) {
-              S.v.mk.m2[r] = om & ~hit;
-              if (dc > 0)
-                S.v.mk.m0[r] |= hit;
-              else
-                S.v.mk.m1[r] |= hit;
-            }
-          }
-          __syncwarp();
-          flood(S, lane);
-        }
-        for (int r = lane; r < 81; r += 32) {
-          uint32_t pm = S.v.mk.m0[r], qm = S.v.mk.m1[r];
-          for (int i = 0; i < 9; i++) {
-            int nn = 9 * r + i;
-            if (!isnan(S.u.f[nn])) continue;
-            if ((pm >> i) & 1u)
-              S.u.f[nn] = clamp;
-            else if ((qm >> i) & 1u)
-              S.u.f[nn] = -clamp;
-          }
-        }
-      }
-      __syncwarp();
-      // ---- bridging: the mean of the known neighbours, held in the brackets the exact
-      // ones give (partcache.rs:893-916), pass after pass; m0 the nodes known when the
-      // pass began, m1 the nodes it sets
-      for (int r = lane; r < 81; r += 32) {
-        uint32_t km = 0;
-        for (int i = 0; i < 9; i++)
-          if (!isnan(S.u.f[9 * r + i])) km |= 1u << i;
-        S.v.mk.m0[r] = km;
-      }
-      __syncwarp();
-      for (int pass = 0; pass < 729; pass++) {
-        bool any = false;
-        for (int r = lane; r < 81; r += 32) {
-          uint32_t sm = dilate_row(S.v.mk.m0, r) & ~S.v.mk.m0[r] & 0x1ffu;
-          S.v.mk.m1[r] = sm;
-          any |= sm != 0;
-        }
-        if (!__any_sync(FULL, any)) break;
-        __syncwarp();
-        for (int nn = lane; nn < 729; nn += 32) {
-          if (!((S.v.mk.m1[nn / 9] >> (nn % 9)) & 1u)) continue;
-          double sum = 0.0, lo = -clamp, hi = clamp;
-          int cn = 0;
-          for (int k = 0; k < 26; k++) {
-            double dd;
-            int m = nb_of(nn, k, &dd);
-            if (m < 0) continue;
-            if ((S.v.mk.m0[m / 9] >> (m % 9)) & 1u) {
-              sum += S.u.f[m];
-              cn++;
-              if (S.flag[m] == 0) {
-                lo = fmax(lo, S.u.f[m] - dd * h);
-                hi = fmin(hi, S.u.f[m] + dd * h);
-              }
-            }
-          }
-          double vm = sum / cn;
-          S.u.f[nn] = lo <= hi ? fmin(fmax(vm, lo), hi) : 0.5 * (lo + hi);
-          provisional++;
-        }
-        __syncwarp();
-        for (int r = lane; r < 81; r += 32) S.v.mk.m0[r] |= S.v.mk.m1[r];
-        __syncwarp();
-      }
-      // nothing around them known: the brick's far side, taken as air
-      for (int nn = lane; nn < 729; nn += 32)
-        if (isnan(S.u.f[nn])) {
-          S.u.f[nn] = clamp;
-          provisional++;
-        }
-      __syncwarp();
-      // ---- quantise and pack
-      bool pos = true, nonpos = true;
-      for (int w = lane; w < 365; w += 32) {
-        double q0 = round(fmin(fmax(S.u.f[2 * w] / clamp, -1.0), 1.0) * 32767.0);
-        pos = pos && q0 > 0;
-        nonpos = nonpos && q0 <= 0;
-        uint32_t word = uint32_t(uint16_t(int16_t(q0)));
-        if (2 * w + 1 < 729) {
-          double q1 = round(fmin(fmax(S.u.f[2 * w + 1] / clamp, -1.0), 1.0) * 32767.0);
-          pos = pos && q1 > 0;
-          nonpos = nonpos && q1 <= 0;
-          word |= uint32_t(uint16_t(int16_t(q1))) << 16;
-        }
-        if (a.words_out) a.words_out[bi * 365 + w] = word;
-      }
-      const bool all_pos = __all_sync(FULL, pos), all_nonpos = __all_sync(FULL, nonpos);
-      if (a.kind_out && lane == 0) a.kind_out[bi] = all_pos ? 1 : (all_nonpos ? 2 : 0);
-    }
-    if (a.stats) {
-      provisional = __reduce_add_sync(FULL, provisional);
-      // the census by kind, B-spline sub-patches counted by their distinct spans
-      unsigned kinds[5] = {0, 0, 0, 0, 0};
-      for (int k = lane; k < n; k += 32) {
-        uint32_t kind = S.code[k] >> IK_SHIFT;
-        if (kind == IK_SUB) {
-          const DSub& s = P.subs[S.code[k] & IK_MASK];
-          bool seen = false;
-          for (int j = 0; j < k && !seen; j++)
-            if ((S.code[j] >> IK_SHIFT) == IK_SUB) {
-              const DSub& o = P.subs[S.code[j] & IK_MASK];
-              seen = o.nurbs == s.nurbs && o.span_a == s.span_a && o.span_b == s.span_b;
-            }
-          if (!seen) kinds[1]++;
-        } else {
-          kinds[kind == IK_FACE ? 0 : kind == IK_EDGE ? 2 : kind == IK_PIECE ? 3 : 4]++;
-        }
-      }
-      for (int k = 0; k < 5; k++) kinds[k] = __reduce_add_sync(FULL, kinds[k]);
-      if (lane == 0) {
-        atomicAdd(&a.stats[0], (unsigned long long)n_exact);
-        atomicAdd(&a.stats[1], (unsigned long long)n_far);
-        atomicAdd(&a.stats[2], (unsigned long long)n_und);
-        if (provisional) atomicAdd(&a.stats[3], (unsigned long long)provisional);
-        atomicAdd(&a.stats[4], (unsigned long long)n);
-        for (int k = 0; k < 5; k++)
-          if (kinds[k]) atomicAdd(&a.stats[6 + k], (unsigned long long)kinds[k]);
-        if (overflow) atomicAdd(&a.stats[5], 1ull);
-      }
-    }
+    if (a.words_out || a.kind_out)
+      provisional = brick_post<double>(S.u.f, S.flag, S.v.mk, first, h, clamp, dc, 0.0, n_far,
+                                       a.words_out ? a.words_out + bi * 365 : nullptr,
+                                       a.kind_out ? a.kind_out + bi : nullptr, lane);
+    if (a.stats) brick_census(P, S.code, n, overflow, n_exact, n_far, n_und, provisional, a.stats, lane);
     __syncwarp();
   }
 }
@@ -466,17 +241,11 @@ void launch_bricks(const BrickArgs& a, cudaStream_t s, int warps) {
   const int grid = int(std::max<int64_t>(1, std::min<int64_t>(want, int64_t(sms) * (8 / warps))));
   const size_t smem = sizeof(BrickSmem) * warps;
   const bool batch = a.parts != nullptr;
-  if (a.mixed) {
-    if (batch)
-      k_bricks_t<true, true><<<grid, warps * 32, smem, s>>>(a);
-    else
-      k_bricks_t<true, false><<<grid, warps * 32, smem, s>>>(a);
-  } else {
-    if (batch)
-      k_bricks_t<false, true><<<grid, warps * 32, smem, s>>>(a);
-    else
-      k_bricks_t<false, false><<<grid, warps * 32, smem, s>>>(a);
-  }
+  if (a.mixed) return launch_bricks_mixed(a, s, warps);
+  if (batch)
+    k_bricks_t<false, true><<<grid, warps * 32, smem, s>>>(a);
+  else
+    k_bricks_t<false, false><<<grid, warps * 32, smem, s>>>(a);
 }
 
 }  // namespace icam

@@ -2,6 +2,7 @@
 // centres read through one shared candidate list, each box then decided air or material,
 // split, or (size 1) read.
 #include "kernels.h"
+#include "warp_float.cuh"
 #include "warp_list.cuh"
 
 namespace icam {
@@ -33,15 +34,18 @@ static_assert(sizeof(DecideSmem) * DWARPS <= 48 * 1024, "static shared memory of
 // One box's verdict from its centre's value (v, f) read within `cut` (partcache.rs:370-383:
 // decided once the centre is known past the box grown by the clamp), the map entries it
 // settles, and its children (up to 8: into kids, *nk of them, for the caller to append;
-// appended here together when kids is null) or its read.
+// appended here together when kids is null) or its read. verr: v's error bound (0 for a
+// double reading; the float reading's caller has made sure the verdict does not lie
+// within it), which the sign and bounds handed to the children and the read bricks
+// allow for, so that the map is the exact reading's.
 __device__ void decide_box(const DecideArgs& a, long long size, const Box4& b, double3 c, double r, double cut,
-                           double v, int f, Box4* kids_out = nullptr, int* nk_out = nullptr) {
+                           double v, int f, Box4* kids_out = nullptr, int* nk_out = nullptr, double verr = 0.0) {
   const DPack& P = a.P;
   const double side = 8.0 * a.h;
-  double sd = NAN;  // the signed distance at the centre when known
+  double sd = NAN;  // the signed distance at the centre when known (its sign sure)
   int verdict;      // 0 split or read, 1 air, 2 material
   if (f == 0) {
-    sd = v;
+    sd = fabs(v) > verr ? v : NAN;
     verdict = (v - r > a.clamp) ? 1 : ((v + r < -a.clamp) ? 2 : 0);
   } else if (f == 1) {
     // past the box: air or material as the parent's centre when the parent's centre lies
@@ -72,7 +76,9 @@ __device__ void decide_box(const DecideArgs& a, long long size, const Box4& b, d
     unsigned long long slot = atomicAdd(a.n_read, 1ull);
     if (slot < (unsigned long long)a.read_cap) {
       a.read_idx[slot] = idx;
-      a.read_dc[slot] = sd;
+      // a float reading hands on a lower bound of |sd| with its sign: the brick kernel's
+      // shortcuts and its centre ball read the centre distance as a bound
+      a.read_dc[slot] = isfinite(sd) ? copysign(fabs(sd) - verr, sd) : sd;
     }
   } else {
     const long long half = size / 2;
@@ -84,7 +90,7 @@ __device__ void decide_box(const DecideArgs& a, long long size, const Box4& b, d
     // |sd| - reach (a bound on |v| with sd's sign) already settles the brick by sign, the
     // brick kernel needs nothing more of it. Such a child is read with that bound as its
     // centre distance instead of being queried.
-    const bool by_bound = half == 1 && isfinite(sd) && sd != 0.0;
+    const bool by_bound = half == 1 && isfinite(sd) && sd != 0.0 && fabs(sd) > verr;
     for (int q = 0; q < 8; q++) {
       Box4 k;
       k.x = b.x + half * (q & 1);
@@ -98,9 +104,9 @@ __device__ void decide_box(const DecideArgs& a, long long size, const Box4& b, d
       k.parent_sd = sd;
       if (by_bound) {
         const double rk = 0.5 * len(khi - klo);
-        const double bound = fabs(sd) - k.reach;
+        const double bound = fabs(sd) - verr - k.reach;
         const double dcb = copysign(bound, sd);
-        if (fabs(sd) + k.reach < (rk + a.clamp) * (1.0 - 1e-12) && bound > 0.0 &&
+        if (fabs(sd) + verr + k.reach < (rk + a.clamp) * (1.0 - 1e-12) && bound > 0.0 &&
             settles_by_sign(dcb, a.h, a.clamp, 1e-9 * (1.0 + a.clamp))) {
           const long long idx = k.x + nb0 * (k.y + nb1 * k.z);
           a.map[idx] = 0xfffffff0u;  // read
@@ -208,6 +214,160 @@ __device__ __forceinline__ void decide_group(const DecideArgs& a, const Box4* bo
   __syncwarp();
 }
 
+// decide_group in the mixed form: the group's list ranked in double as there, then every
+// centre read by the float walk (warp_float.cuh) over candidates certified for the whole
+// group (sub-patches convex over the box of the group's centres, planes' trims over their
+// feet), seeded in floats at the group's centre. A centre the float walk cannot settle,
+// or whose verdict lies within the float error of its threshold (|v| = r + clamp), is
+// read again by the double walk; the rest are decided on the float value, whose error
+// bound decide_box allows for. The map is the double reading's.
+struct DecideSmemF {
+  union {
+    struct {
+      uint32_t tcode[DMAXC];  // the list before its ranking, and the walk's frontier
+      double tlb[DMAXC];
+      int32_t fr[2][FR];
+    } list;
+    float4 geo[2 * DMAXC];  // after the ranking: the candidates' float geometry
+  } u;
+  double lb[DMAXC];  // ranked candidates
+  float lbf[DMAXC];
+  uint32_t code[DMAXC];
+  SeedF seed[MAXSUB];
+  double4 net[16];
+  float4 net32[16];
+  int8_t cert[DMAXC];
+  int8_t slot[DMAXC];
+  int n;
+};
+
+__device__ __forceinline__ void decide_group_f(const DecideArgs& a, const Box4* boxes, int64_t n, long long size,
+                                               int64_t g0, int gs, DecideSmemF& S, int lane, bool first) {
+  const DPack& P = a.P;
+  const double side = 8.0 * a.h;
+  const int64_t i = g0 + lane;
+  const bool live = lane < gs && i < n;
+  const Box4 b = boxes[live ? i : g0];
+  double3 lo = mk(a.lo[0] + side * b.x - a.clamp, a.lo[1] + side * b.y - a.clamp, a.lo[2] + side * b.z - a.clamp);
+  double3 hi = mk(a.lo[0] + side * (b.x + size) + a.clamp, a.lo[1] + side * (b.y + size) + a.clamp,
+                  a.lo[2] + side * (b.z + size) + a.clamp);
+  const double3 c = (lo + hi) * 0.5;
+  const double r = 0.5 * len(hi - lo);
+  const double cut = (r + a.clamp) * (1.0 + 1e-4);
+  double bl[3] = {c.x, c.y, c.z}, bh[3] = {c.x, c.y, c.z};
+  for (int o = 16; o > 0; o >>= 1)
+    for (int k = 0; k < 3; k++) {
+      bl[k] = fmin(bl[k], __shfl_xor_sync(FULL, bl[k], o));
+      bh[k] = fmax(bh[k], __shfl_xor_sync(FULL, bh[k], o));
+    }
+  const double3 gc = mk(0.5 * (bl[0] + bh[0]), 0.5 * (bl[1] + bh[1]), 0.5 * (bl[2] + bh[2]));
+  double R = len(c - gc);
+  for (int o = 16; o > 0; o >>= 1) R = fmax(R, __shfl_xor_sync(FULL, R, o));
+  int nc = warp_list<DMAXC>(P, a.leaves, a.n_leaves, gc, R + cut, S.u.list.tcode, S.u.list.tlb, S.u.list.fr, &S.n,
+                            lane);
+  const bool overflow = nc > DMAXC;
+  if (overflow) nc = DMAXC;
+  warp_rank(S.u.list.tcode, S.u.list.tlb, nc, S.code, S.lb, lane);
+  const double3 blo = mk(bl[0], bl[1], bl[2]), bhi = mk(bh[0], bh[1], bh[2]);
+  int subs_before = 0;
+  for (int base = 0; base < nc; base += 32) {
+    const int k = base + lane;
+    const bool is_sub = k < nc && (S.code[k] >> IK_SHIFT) == IK_SUB;
+    const unsigned m = __ballot_sync(FULL, is_sub);
+    const int before = subs_before + __popc(m & ((1u << lane) - 1u));
+    subs_before += __popc(m);
+    if (k >= nc) continue;
+    const uint32_t code = S.code[k], idx = code & IK_MASK;
+    int slot = -1;
+    int8_t cert = 0;
+    float4 g0v = make_float4(0.f, 0.f, 0.f, 0.f), g1v = g0v;
+    S.lbf[k] = __double2float_rd(S.lb[k]);
+    if (is_sub) {
+      const DSub& s = P.subs[idx];
+      cert = sub_convex(s, blo, bhi) ? 1 : 0;
+      g0v = make_float4(float(s.c[0] - gc.x), float(s.c[1] - gc.y), float(s.c[2] - gc.z), float(P.faces[s.face].sense));
+      g1v = make_float4(__double2float_ru(0.5 * (s.box[3] - s.box[0])), __double2float_ru(0.5 * (s.box[4] - s.box[1])),
+                        __double2float_ru(0.5 * (s.box[5] - s.box[2])), 0.f);
+      if (before < MAXSUB) {
+        slot = before;
+        const float3 qc = f3(float(gc.x - s.c[0]), float(gc.y - s.c[1]), float(gc.z - s.c[2]));
+        S.seed[slot] = seed_at_f(P.sub_cp32 + 16 * size_t(idx), qc, 0.5f, 0.5f);
+      }
+    } else if ((code >> IK_SHIFT) == IK_FACE) {
+      const DFace& f = P.faces[idx];
+      if (f.kind == S_PLANE) {
+        const double3 z = ld3(f.z) * f.sense, o = ld3(f.o);
+        g0v = make_float4(float(z.x), float(z.y), float(z.z), float(dot(o - gc, z)));
+        double tlo[2] = {INFINITY, INFINITY}, thi[2] = {-INFINITY, -INFINITY};
+        const double3 zz = ld3(f.z), fx = ld3(f.x), fy = ld3(f.y);
+        for (int q = 0; q < 8; q++) {
+          double3 x = mk(q & 1 ? bh[0] : bl[0], q & 2 ? bh[1] : bl[1], q & 4 ? bh[2] : bl[2]);
+          double3 e = (x - zz * dot(x - o, zz)) - o;
+          double u = dot(e, fx), v = dot(e, fy);
+          tlo[0] = fmin(tlo[0], u), thi[0] = fmax(thi[0], u);
+          tlo[1] = fmin(tlo[1], v), thi[1] = fmax(thi[1], v);
+        }
+        double mg = 1e-9 * (1.0 + fmax(fmax(fabs(tlo[0]), fabs(thi[0])), fmax(fabs(tlo[1]), fabs(thi[1]))));
+        tlo[0] -= mg, tlo[1] -= mg, thi[0] += mg, thi[1] += mg;
+        const int cls = trim_box_class(P, f, tlo, thi);
+        cert = cls == 1 ? 1 : (cls == 0 ? 2 : 0);
+      } else {
+        g0v.w = NAN;
+      }
+    }
+    S.u.geo[2 * k] = g0v;
+    S.u.geo[2 * k + 1] = g1v;
+    S.cert[k] = cert;
+    S.slot[k] = int8_t(slot);
+  }
+  __syncwarp();
+  float vf = 0.f;
+  int f = 3;
+  if (!overflow) {
+    const WarpCandsF W{S.code, S.lbf, S.cert, S.slot, S.seed, S.u.geo, S.net32, nc};
+    int lastk = -1;
+    float ls = 0.f, lt = 0.f;
+    f = warp_point_f(P, W, f3(float(c.x - gc.x), float(c.y - gc.y), float(c.z - gc.z)), c, live, float(cut), lane,
+                     &vf, &lastk, &ls, &lt);
+  }
+  double v = vf, verr = 0.0;
+  if (f == 0) {
+    verr = 1e-4 + 4e-6 * (fabs(v) + R);
+    if (fabs(fabs(v) - (r + a.clamp)) <= verr) f = 3;  // the verdict is within the float error
+  }
+  const bool pd = live && f == 3;
+  if (__any_sync(FULL, pd)) {  // the double walk over the same candidates, centre starts
+    const WarpCands W64{S.code, S.lb, S.cert, nullptr, nullptr, S.net, S.net32, nc, overflow};
+    double v64;
+    int f64;
+    warp_point<false>(P, W64, c, gc, pd, cut, lane, &v64, &f64);
+    if (pd) v = v64, f = f64, verr = 0.0;
+    if (a.n_double && pd) atomicAdd(a.n_double, 1ull);
+  }
+  Box4 kids[8];
+  int nk = 0;
+  if (live) {
+    if (first) {
+      a.first_sd[i] = f == 0 ? v : NAN;
+      a.first_sign[i] = f == 1 ? FS_PENDING : ((f == 0 && fabs(v) > verr && v != 0.0) ? (v > 0 ? 1 : -1) : 0);
+    }
+    if (!(first && f == 1)) decide_box(a, size, b, c, r, cut, v, f, kids, &nk, verr);
+  }
+  int incl = nk;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(FULL, incl, o);
+    if (lane >= o) incl += t;
+  }
+  const int total = __shfl_sync(FULL, incl, 31);
+  unsigned long long base = 0;
+  if (lane == 31 && total > 0) base = atomicAdd(a.n_next, (unsigned long long)total);
+  base = __shfl_sync(FULL, base, 31);
+  const unsigned long long off = base + (unsigned long long)(incl - nk);
+  for (int q = 0; q < nk; q++)
+    if (off + q < (unsigned long long)a.next_cap) a.next[off + q] = kids[q];
+  __syncwarp();
+}
+
 // The centre, radius and cut of a box of `size` bricks (as decide_group computes them).
 __device__ __forceinline__ void box_geometry(const DecideArgs& a, const Box4& b, long long size, double3* c, double* r,
                                              double* cut) {
@@ -298,6 +458,16 @@ __global__ void __launch_bounds__(DWARPS * 32, 2) k_decide_w(DecideArgs a, int g
     decide_group(a, a.boxes, a.n, a.size, g0, gs, smem[warp], lane, a.first_sd != nullptr);
 }
 
+// The mixed form's decision of one box size: three blocks a SM (the float walk's
+// registers), the groups' room in dynamic shared memory.
+__global__ void __launch_bounds__(DWARPS * 32, 3) k_decide_wf(DecideArgs a, int gs) {
+  extern __shared__ __align__(16) unsigned char dsm[];
+  DecideSmemF* smem = reinterpret_cast<DecideSmemF*>(dsm);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int64_t g0 = (int64_t(blockIdx.x) * DWARPS + warp) * gs; g0 < a.n; g0 += int64_t(gridDim.x) * DWARPS * gs)
+    decide_group_f(a, a.boxes, a.n, a.size, g0, gs, smem[warp], lane, a.first_sd != nullptr);
+}
+
 // A batch's round (one box size a part): the counts the last round appended become this
 // round's, the next counts start at zero, and the parts' groups of 32 are numbered.
 // One thread: a batch holds tens to thousands of parts.
@@ -329,8 +499,9 @@ __global__ void k_decide_prep(DecideBatchArgs b, int round) {
 
 // A batch's round: every part's boxes of this round's size, 32 of one part a warp, the
 // warps taking groups across all parts from the numbering k_decide_prep made.
-__global__ void __launch_bounds__(DWARPS * 32, 2) k_decide_batch(DecideBatchArgs b, int round) {
-  __shared__ DecideSmem smem[DWARPS];
+template <bool F32>
+__global__ void __launch_bounds__(DWARPS * 32, F32 ? 3 : 2) k_decide_batch(DecideBatchArgs b, int round) {
+  extern __shared__ __align__(16) unsigned char dsm[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t total = b.groups[b.n_parts];
   const int gs = int(b.groups[b.n_parts + 1]);
@@ -343,7 +514,12 @@ __global__ void __launch_bounds__(DWARPS * 32, 2) k_decide_batch(DecideBatchArgs
     }
     const DecideArgs& a = b.args[2 * lo + (round & 1)];
     const int64_t n = int64_t(b.cnt[2 * lo + (round & 1)]);
-    decide_group(a, a.boxes, n, a.size >> round, (g - b.groups[lo]) * gs, gs, smem[warp], lane, round == 0);
+    if (F32)
+      decide_group_f(a, a.boxes, n, a.size >> round, (g - b.groups[lo]) * gs, gs,
+                     reinterpret_cast<DecideSmemF*>(dsm)[warp], lane, round == 0);
+    else
+      decide_group(a, a.boxes, n, a.size >> round, (g - b.groups[lo]) * gs, gs,
+                   reinterpret_cast<DecideSmem*>(dsm)[warp], lane, round == 0);
   }
 }
 
@@ -353,13 +529,20 @@ __global__ void __launch_bounds__(256) k_first_signs_batch(DecideBatchArgs b) {
   first_signs(b.args[2 * p], int64_t(b.cnt[2 * p]));
 }
 
-void launch_decide(const DecideArgs& a, cudaStream_t s, bool first) {
+void launch_decide(const DecideArgs& a, cudaStream_t s, bool first, bool mixed) {
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int per_sm = mixed ? 3 : 2;
   const int gs = group_size(a.n, sms);
   const int64_t want = (a.n + DWARPS * gs - 1) / (DWARPS * gs);
-  const int grid = int(std::max<int64_t>(1, std::min<int64_t>(want, int64_t(sms) * 2)));
-  k_decide_w<<<grid, DWARPS * 32, 0, s>>>(a, gs);
+  const int grid = int(std::max<int64_t>(1, std::min<int64_t>(want, int64_t(sms) * per_sm)));
+  if (mixed) {
+    const size_t smem = sizeof(DecideSmemF) * DWARPS;
+    cudaFuncSetAttribute(k_decide_wf, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    k_decide_wf<<<grid, DWARPS * 32, smem, s>>>(a, gs);
+  } else {
+    k_decide_w<<<grid, DWARPS * 32, 0, s>>>(a, gs);
+  }
   if (first) k_first_signs<<<1, 256, 0, s>>>(a, a.n);
 }
 
@@ -368,9 +551,14 @@ void launch_decide_batch(const DecideBatchArgs& b, int rounds, cudaStream_t s) {
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   DecideBatchArgs bb = b;
   bb.sms = sms;
+  const size_t smem = b.mixed ? sizeof(DecideSmemF) * DWARPS : sizeof(DecideSmem) * DWARPS;
+  if (b.mixed) cudaFuncSetAttribute(k_decide_batch<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   for (int r = 0; r < rounds; r++) {
     k_decide_prep<<<1, 32, 0, s>>>(bb, r);
-    k_decide_batch<<<sms * 2, DWARPS * 32, 0, s>>>(bb, r);
+    if (b.mixed)
+      k_decide_batch<true><<<sms * 3, DWARPS * 32, smem, s>>>(bb, r);
+    else
+      k_decide_batch<false><<<sms * 2, DWARPS * 32, smem, s>>>(bb, r);
     if (r == 0) k_first_signs_batch<<<b.n_parts, 256, 0, s>>>(bb);
   }
 }

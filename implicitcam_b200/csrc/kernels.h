@@ -35,6 +35,7 @@ struct BrickArgs {
   DPack P;
   const double* firsts;  // n x 3 first nodes
   const double* dcs;     // n centre distances (NaN when not known), or null
+  double dc_err;         // the centre distances' error bound (0: exact; the mixed decision's float reading)
   int64_t n;
   double h, clamp;
   const int32_t* leaves;  // the tree's leaf nodes
@@ -49,8 +50,9 @@ struct BrickArgs {
   uint32_t* words_out;    // optional n x 365 packed words
   int32_t* kind_out;      // optional n kinds (0 words, 1 air, 2 solid)
   // exact, far, undecided, bridged, pairs, overflows, census [6..10], bricks given their
-  // kind from the centre alone [11]; [15] the kernel's brick counter. Zeroed before each launch; null for none (bricks then taken in a
-  // fixed order).
+  // kind from the centre alone [11], nodes the mixed kernel read in double precision [12];
+  // [15] the kernel's brick counter. Zeroed before each launch; null for none (bricks
+  // then taken in a fixed order).
   unsigned long long* stats;
 };
 
@@ -77,6 +79,8 @@ struct DecideArgs {
   double* first_sd;
   int8_t* first_sign;
   long long first_dims[3];
+  // the mixed form: centres the float walk left to the double walk (counted; or null)
+  unsigned long long* n_double;
 };
 
 __global__ void k_points(DPack P, const double* xyz, int64_t n, double cap, double* value, int8_t* flag);
@@ -84,13 +88,17 @@ __global__ void k_points(DPack P, const double* xyz, int64_t n, double cap, doub
 // The brick kernel (bricks.cu) in the arithmetic a.mixed names, one warp a brick, `warps`
 // (1, 2 or 4) a block, over a grid sized for the current device.
 void launch_bricks(const BrickArgs& a, cudaStream_t s, int warps = 4);
+// The mixed form's brick kernel (bricks_mixed.cu): float bulk, the nodes it cannot settle
+// read by the double walk afterwards; launch_bricks sends a.mixed here.
+void launch_bricks_mixed(const BrickArgs& a, cudaStream_t s, int warps = 4);
 // Map entries and atlas words of a batch's read bricks (batch.cu).
 __global__ void k_assemble_batch(const int64_t* idx, const int32_t* part_of, const int64_t* part_off,
                                  uint32_t* const* maps, const int32_t* kind, const int64_t* slot, int64_t n,
                                  const uint32_t* words, uint32_t* atlas);
 // The decision of one box size of a level (decide.cu), 32 boxes a warp; `first`: the
 // level's first boxes, whose far ones then take their sign from a neighbour.
-void launch_decide(const DecideArgs& a, cudaStream_t s, bool first = false);
+// mixed: the float reading (decide.cu decide_group_f), the same map.
+void launch_decide(const DecideArgs& a, cudaStream_t s, bool first = false, bool mixed = false);
 
 // Many parts' decisions together (decide.cu), one round a box size. Part p's fields are
 // args[2p + (round & 1)]: `size` its first boxes' size (round r decides size >> r),
@@ -106,6 +114,7 @@ struct DecideBatchArgs {
   int64_t* groups;
   unsigned long long* boxes_read;
   int* err;  // set when a part's box list would overflow
+  int mixed;  // the float reading (decide_group_f)
 };
 // `rounds` rounds (the largest first box size's log2 + 1), no host synchronisation.
 void launch_decide_batch(const DecideBatchArgs& b, int rounds, cudaStream_t s);

@@ -47,6 +47,7 @@ struct DecideOut {
   double* read_dc = nullptr;
   int64_t n_read = 0, boxes_read = 0, launches = 0;
   int64_t h2d_bytes = 0, d2h_bytes = 0;  // host copies the decision made
+  int64_t centres_double = 0;            // the mixed form: box centres read again in double
 };
 
 namespace icam {

@@ -217,7 +217,8 @@ static __device__ __noinline__ bool sub_convex_at(const DSub& s, double3 p) { re
 // A warp's ranked candidates, in shared memory: code and bound at the centre c, a
 // verdict per candidate (sub-patch: 1 convex over every point the warp asks about;
 // plane: 1 its trim holds at every foot, 2 at none; else 0), the seed slot of each
-// sub-patch (-1 none), and room for the control net the warp is on.
+// sub-patch (-1 none; slot null: no seeds, every solve starts at the centre), and room
+// for the control net the warp is on.
 struct WarpCands {
   const uint32_t* code;
   const double* lb;
@@ -304,7 +305,7 @@ __device__ __forceinline__ void warp_point(const DPack& P, const WarpCands& W, d
       defer_item(code, lb);
       continue;
     }
-    const int slot = W.slot[k];
+    const int slot = W.slot ? W.slot[k] : -1;
     double ss = 0.5, tt = 0.5;
     if (slot >= 0) seed_params(W.seed[slot], p - c, &ss, &tt);
     const double4* cp64 = W.net;

@@ -84,6 +84,12 @@ typedef struct IcamBakeStats {
   /* Bytes the call copied from host to device (the decision's first boxes) and from
    * device to host (its counts, and for icam_bake_level the map and atlas). */
   int64_t h2d_bytes, d2h_bytes;
+  /* The mixed forms: nodes the single-precision walk left to the double walk (a
+   * distance near zero, a stalled or uncertified solve, a deferred feature). */
+  int64_t nodes_double;
+  /* The mixed forms: box centres the decision's float reading left to the double walk
+   * (a verdict within the float error of its threshold, a value near zero). */
+  int64_t centres_double;
 } IcamBakeStats;
 
 /* Packs the solid for the device (PartGpu::new, partgpu.rs:132; Exact::gpu_pack,

@@ -94,8 +94,12 @@ def test_learned_brick_values(torch_cuda, oracle_mod, name):
     ex = flag == 0
     assert (flag != 2).all()
     assert np.abs(d[ex] - fo[ex]).max() <= TOL_MIXED * diag
-    nz = ex & (fo != 0)
-    assert (np.sign(d[nz]) == np.sign(fo[nz])).all()
+    # signs wherever the distance is above double rounding (a node on the surface up to
+    # rounding has a sign of rounding; the reference's verify compares signs only past
+    # the i16 step of zero, partcache.rs:536-538)
+    nz = ex & (np.abs(fo) > 1e-9)
+    bad = nz & (np.sign(d) != np.sign(fo))
+    assert not bad.any(), (fo[bad][:5], d[bad][:5])
     assert (np.abs(fo[flag == 1]) >= clamp * (1 - 1e-12)).all()
 
 
