@@ -255,9 +255,12 @@ int icam_bricks(IcamPack* pk, const double* first_nodes, size_t n, double h, dou
   CK(cudaGetLastError());
   std::vector<double> v(n * 729);
   std::vector<int8_t> f(n * 729);
+  unsigned long long st[16];
   CK(cudaMemcpyAsync(v.data(), dval, n * 729 * sizeof(double), cudaMemcpyDeviceToHost, pk->stream));
   CK(cudaMemcpyAsync(f.data(), dflag, n * 729, cudaMemcpyDeviceToHost, pk->stream));
+  CK(cudaMemcpyAsync(st, pk->d_stats, sizeof(st), cudaMemcpyDeviceToHost, pk->stream));
   CK(cudaStreamSynchronize(pk->stream));
+  if (st[13]) return fail(pk, ICAM_ERR_BUDGET, "a bulk copy of control nets did not complete in time");
   for (size_t i = 0; i < n * 729; i++) {
     if (values_out) {
       values_out[2 * i] = float(v[i]);
@@ -501,9 +504,13 @@ static int bake_level(IcamPack* pk, double h, const double lo[3], const int64_t 
   pk->last_atlas = (const uint32_t*)d_atlas;
   pk->last_map_entries = size_t(nb[0] * nb[1] * nb[2]);
   pk->last_slots = nwords_slots;
+  unsigned long long st[16] = {0};
+  if (R > 0) CK(cudaMemcpy(st, pk->d_stats, sizeof(st), cudaMemcpyDeviceToHost));
+  if (st[13]) {
+    for (auto& e : ev) cudaEventDestroy(e);
+    return fail(pk, ICAM_ERR_BUDGET, "a bulk copy of control nets did not complete in time");
+  }
   if (stats) {
-    unsigned long long st[16] = {0};
-    CK(cudaMemcpy(st, pk->d_stats, sizeof(st), cudaMemcpyDeviceToHost));
     std::memset(stats, 0, sizeof(*stats));
     stats->boxes_read = boxes_read;
     stats->bricks_read = R;

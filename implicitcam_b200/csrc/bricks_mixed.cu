@@ -20,14 +20,19 @@ constexpr int SN_ROOM = 32 * SN_KS * 2 + 32 * 8 * 4;  // the seed network's acti
 
 struct BrickSmemF {
   union {
-    float f[729];  // node values: exact, signed far, bridged; NaN while unknown
     struct {
-      uint32_t code[MAXC];
-      double lb[MAXC];
-      int32_t fr[2][FR];
-    } list;
-    unsigned char net[SN_ROOM];
-  } u;
+      union {
+        float f[729];  // node values: exact, signed far, bridged; NaN while unknown
+        struct {
+          uint32_t code[MAXC];
+          double lb[MAXC];
+          int32_t fr[2][FR];
+        } list;
+      } u;
+      float4 res[16 * NRES];  // the resident nets (staged after the seed network has run)
+    } w;
+    unsigned char net[SN_ROOM];  // the seed network's activations, before the nets come
+  } x;
   double lb64[MAXC];  // ranked candidates: lower bound at the centre (double, then float
   float lbf[MAXC];    //   rounded down), code, float geometry (WarpCandsF)
   uint32_t code[MAXC];
@@ -42,8 +47,12 @@ struct BrickSmemF {
   int8_t flag[729];
   int8_t cert[MAXC];
   int8_t slot[MAXC];
+  int8_t rslot[MAXC];
+  uint32_t residx[NRES];
+  uint64_t bar;  // the bulk copies' barrier
   int n;
 };
+static_assert(sizeof(((BrickSmemF*)0)->x) >= SN_ROOM, "the seed network's room");
 
 // The i16 step's half: a distance below it (less the float error) rounds to zero on
 // either side of the surface, so a bake that keeps only i16 values needs no sign for it.
@@ -66,13 +75,16 @@ __device__ __forceinline__ float quantised_zero(double clamp) {
 //  4. the nodes left over, 32 at a time, by the plain form's double walk;
 //  5. far nodes signed, undecided ones bridged, quantised and packed.
 template <bool BATCH>
-__global__ void __launch_bounds__(MW * 32, 3) k_bricks_m(BrickArgs a) {
+__global__ void __launch_bounds__(MW * 32, ICAM_MIXED_BLOCKS) k_bricks_m(BrickArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   BrickSmemF* smem = reinterpret_cast<BrickSmemF*>(smem_raw);
   const int warps = int(blockDim.x >> 5);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   BrickSmemF& S = smem[warp];
   unsigned long long* work = a.stats ? a.stats + 15 : nullptr;
+  if (lane == 0) mbar_init(&S.bar);
+  __syncwarp();
+  uint32_t phase = 0;
   auto next_brick = [&](int64_t cur) -> int64_t {
     if (work) {
       unsigned long long b = 0;
@@ -119,10 +131,10 @@ __global__ void __launch_bounds__(MW * 32, 3) k_bricks_m(BrickArgs a) {
       continue;
     }
     // ---- 1. list
-    int n = warp_list(P, leaves, n_leaves, c, reach, S.u.list.code, S.u.list.lb, S.u.list.fr, &S.n, lane);
+    int n = warp_list(P, leaves, n_leaves, c, reach, S.x.w.u.list.code, S.x.w.u.list.lb, S.x.w.u.list.fr, &S.n, lane);
     const bool overflow = n > MAXC;
     if (overflow) n = MAXC;
-    warp_rank(S.u.list.code, S.u.list.lb, n, S.code, S.lb64, lane);
+    warp_rank(S.x.w.u.list.code, S.x.w.u.list.lb, n, S.code, S.lb64, lane);
     // ---- 2. per candidate
     {
       int subs_before = 0;
@@ -139,13 +151,13 @@ __global__ void __launch_bounds__(MW * 32, 3) k_bricks_m(BrickArgs a) {
           float x[SN_IN], y[3];
           const int fi = is_sub ? int(S.code[k] & IK_MASK) : 0;
           sn_input(net_feat + size_t(fi) * SN_FEAT, c, x);
-          __nv_bfloat16* act = reinterpret_cast<__nv_bfloat16*>(S.u.net);
+          __nv_bfloat16* act = reinterpret_cast<__nv_bfloat16*>(S.x.net);
           sn_forward_warp(net_w, act, reinterpret_cast<float*>(act + 32 * SN_KS), x, y, lane);
           s0 = fminf(fmaxf(y[0], 0.f), 1.f), t0 = fminf(fmaxf(y[1], 0.f), 1.f);
         }
         if (k >= n) continue;
         const uint32_t code = S.code[k], idx = code & IK_MASK;
-        int slot = -1;
+        int slot = -1, rslot = -1;
         int8_t cert = 0;
         float4 g0 = make_float4(0.f, 0.f, 0.f, 0.f), g1 = g0;
         S.lbf[k] = __double2float_rd(S.lb64[k]);
@@ -155,7 +167,11 @@ __global__ void __launch_bounds__(MW * 32, 3) k_bricks_m(BrickArgs a) {
           g0 = make_float4(float(s.c[0] - c.x), float(s.c[1] - c.y), float(s.c[2] - c.z), float(P.faces[s.face].sense));
           // half extents rounded up: a lower bound stays a lower bound
           g1 = make_float4(__double2float_ru(0.5 * (s.box[3] - s.box[0])), __double2float_ru(0.5 * (s.box[4] - s.box[1])),
-                           __double2float_ru(0.5 * (s.box[5] - s.box[2])), 0.f);
+                           __double2float_ru(0.5 * (s.box[5] - s.box[2])), s.klass == 1 ? 1.f : 0.f);
+          if (before < NRES) {
+            rslot = before;
+            S.residx[before] = idx;
+          }
           if (before < MAXSUB) {
             slot = before;
             const float3 qc = f3(float(c.x - s.c[0]), float(c.y - s.c[1]), float(c.z - s.c[2]));
@@ -188,6 +204,19 @@ __global__ void __launch_bounds__(MW * 32, 3) k_bricks_m(BrickArgs a) {
         S.geo[2 * k + 1] = g1;
         S.cert[k] = cert;
         S.slot[k] = int8_t(slot);
+        S.rslot[k] = int8_t(rslot);
+      }
+      // the first NRES sub-patches' nets staged into shared memory for the whole brick
+      const int nres = min(subs_before, NRES);
+      __syncwarp();
+      if (nres > 0) {
+        if (lane == 0) stage_nets(S.x.w.res, P.sub_cp32, S.residx, nres, &S.bar);
+        if (!mbar_wait(&S.bar, phase)) {  // never expected: record it, let the copies land, leave
+          if (a.stats && lane == 0) atomicAdd(&a.stats[13], 1ull);
+          mbar_wait(&S.bar, phase);
+          return;
+        }
+        phase ^= 1u;
       }
     }
     __syncwarp();
@@ -195,7 +224,7 @@ __global__ void __launch_bounds__(MW * 32, 3) k_bricks_m(BrickArgs a) {
     int cnt[3] = {0, 0, 0};
     int pending = 0;
     {
-      const WarpCandsF W{S.code, S.lbf, S.cert, S.slot, S.v.seed, S.geo, S.net32, n};
+      const WarpCandsF W{S.code, S.lbf, S.cert, S.slot, S.v.seed, S.geo, S.net32, S.x.w.res, S.rslot, n, 8};
       int lastk = -1;
       float ls = 0.f, lt = 0.f;
       const float hf = float(h);
@@ -218,7 +247,7 @@ __global__ void __launch_bounds__(MW * 32, 3) k_bricks_m(BrickArgs a) {
         }
         if (a.d_out) a.d_out[bi * 729 + nn] = double(v);
         if (a.flag_out) a.flag_out[bi * 729 + nn] = int8_t(f);
-        S.u.f[nn] = f == 0 ? v : NAN;
+        S.x.w.u.f[nn] = f == 0 ? v : NAN;
         cnt[f]++;
       }
     }
@@ -253,7 +282,7 @@ __global__ void __launch_bounds__(MW * 32, 3) k_bricks_m(BrickArgs a) {
         }
         if (a.d_out) a.d_out[bi * 729 + nn] = v;
         if (a.flag_out) a.flag_out[bi * 729 + nn] = int8_t(f);
-        S.u.f[nn] = f == 0 ? float(v) : NAN;
+        S.x.w.u.f[nn] = f == 0 ? float(v) : NAN;
         cnt[f]++;
       }
       __syncwarp();
@@ -269,7 +298,7 @@ __global__ void __launch_bounds__(MW * 32, 3) k_bricks_m(BrickArgs a) {
           if (a.d_out) a.d_out[bi * 729 + nn] = v;
           if (a.flag_out) a.flag_out[bi * 729 + nn] = int8_t(f);
           S.flag[nn] = int8_t(f);
-          S.u.f[nn] = f == 0 ? float(v) : NAN;
+          S.x.w.u.f[nn] = f == 0 ? float(v) : NAN;
           cnt[f]++;
         }
       }
@@ -280,7 +309,7 @@ __global__ void __launch_bounds__(MW * 32, 3) k_bricks_m(BrickArgs a) {
               n_und = __reduce_add_sync(FULL, cnt[2]);
     int provisional = 0;
     if (a.words_out || a.kind_out)
-      provisional = brick_post<float>(S.u.f, S.flag, S.v.mk, first, h, clamp, dc, dce, n_far,
+      provisional = brick_post<float>(S.x.w.u.f, S.flag, S.v.mk, first, h, clamp, dc, dce, n_far,
                                       a.words_out ? a.words_out + bi * 365 : nullptr,
                                       a.kind_out ? a.kind_out + bi : nullptr, lane);
     if (a.stats) brick_census(P, S.code, n, overflow, n_exact, n_far, n_und, provisional, a.stats, lane);

@@ -132,11 +132,32 @@ __device__ void decide_box(const DecideArgs& a, long long size, const Box4& b, d
   }
 }
 
+// The ball of the centres of lanes [l0, l0 + s) that hold a box (in: their live flags):
+// the middle of their centres' box (gc), the farthest centre from it (R), and that box
+// (bl, bh). Every lane calls it; the others take lane l0's centre, which lies inside.
+__device__ __forceinline__ void centres_ball(double3 c, bool in, int l0, int lane, double3* gc, double* R,
+                                             double bl[3], double bh[3]) {
+  const double3 c0 = mk(__shfl_sync(FULL, c.x, l0), __shfl_sync(FULL, c.y, l0), __shfl_sync(FULL, c.z, l0));
+  const double3 cc = in ? c : c0;
+  bl[0] = bh[0] = cc.x, bl[1] = bh[1] = cc.y, bl[2] = bh[2] = cc.z;
+  for (int o = 16; o > 0; o >>= 1)
+    for (int k = 0; k < 3; k++) {
+      bl[k] = fmin(bl[k], __shfl_xor_sync(FULL, bl[k], o));
+      bh[k] = fmax(bh[k], __shfl_xor_sync(FULL, bh[k], o));
+    }
+  *gc = mk(0.5 * (bl[0] + bh[0]), 0.5 * (bl[1] + bh[1]), 0.5 * (bl[2] + bh[2]));
+  double r = len(cc - *gc);
+  for (int o = 16; o > 0; o >>= 1) r = fmax(r, __shfl_xor_sync(FULL, r, o));
+  *R = r;
+}
+
 // gs (1 to 32) boxes of one size from boxes[g0 ..] (n in all), a lane each: their
-// centres' bounding ball, the
-// features within its radius plus the cut of its centre (listed and ranked once,
-// sub-patches seeded there), every centre's value capped at the cut by the shared walk,
-// then each box decided.
+// centres' bounding ball, the features within its radius plus the cut of its centre
+// (listed and ranked once, sub-patches seeded there), every centre's value capped at the
+// cut by the shared walk, then each box decided. A list that holds more features than
+// its room splits the group in halves (down to one box), each half taking its own list:
+// the boxes' readings are the same, and none walks the whole tree alone while a smaller
+// list would do.
 __device__ __forceinline__ void decide_group(const DecideArgs& a, const Box4* boxes, int64_t n, long long size,
                                              int64_t g0, int gs, DecideSmem& S, int lane, bool first) {
   const DPack& P = a.P;
@@ -150,42 +171,48 @@ __device__ __forceinline__ void decide_group(const DecideArgs& a, const Box4* bo
   const double3 c = (lo + hi) * 0.5;
   const double r = 0.5 * len(hi - lo);
   const double cut = (r + a.clamp) * (1.0 + 1e-4);
-  // the group's centre: the middle of its centres' box; its radius, the farthest centre
-  double bl[3] = {c.x, c.y, c.z}, bh[3] = {c.x, c.y, c.z};
-  for (int o = 16; o > 0; o >>= 1)
-    for (int k = 0; k < 3; k++) {
-      bl[k] = fmin(bl[k], __shfl_xor_sync(FULL, bl[k], o));
-      bh[k] = fmax(bh[k], __shfl_xor_sync(FULL, bh[k], o));
+  const int glanes = int(min(int64_t(gs), n - g0));  // lanes of the group holding a box
+  double v = 0.0;
+  int f = 1;
+  for (int l0 = 0, sg = glanes; l0 < glanes;) {
+    sg = min(sg, glanes - l0);
+    const bool mine = lane >= l0 && lane < l0 + sg;
+    double3 gc;
+    double R, bl[3], bh[3];
+    centres_ball(c, mine, l0, lane, &gc, &R, bl, bh);
+    // every feature nearer than the cut to a centre has a bound <= R + cut from gc
+    int nc = warp_list<DMAXC>(P, a.leaves, a.n_leaves, gc, R + cut, S.tcode, S.tlb, S.fr, &S.n, lane);
+    const bool overflow = nc > DMAXC;
+    if (overflow && sg > 1) {
+      sg = (sg + 1) / 2;
+      continue;
     }
-  const double3 gc = mk(0.5 * (bl[0] + bh[0]), 0.5 * (bl[1] + bh[1]), 0.5 * (bl[2] + bh[2]));
-  double R = len(c - gc);
-  for (int o = 16; o > 0; o >>= 1) R = fmax(R, __shfl_xor_sync(FULL, R, o));
-  // every feature nearer than the cut to a centre has a bound <= R + cut from gc
-  int nc = warp_list<DMAXC>(P, a.leaves, a.n_leaves, gc, R + cut, S.tcode, S.tlb, S.fr, &S.n, lane);
-  const bool overflow = nc > DMAXC;
-  if (overflow) nc = DMAXC;
-  warp_rank(S.tcode, S.tlb, nc, S.code, S.lb, lane);
-  int subs_before = 0;
-  for (int base = 0; base < nc; base += 32) {
-    const int k = base + lane;
-    const bool is_sub = k < nc && (S.code[k] >> IK_SHIFT) == IK_SUB;
-    const unsigned m = __ballot_sync(FULL, is_sub);
-    const int before = subs_before + __popc(m & ((1u << lane) - 1u));
-    subs_before += __popc(m);
-    if (k >= nc) continue;
-    int slot = -1;
-    if (is_sub && before < MAXSUB) {
-      slot = before;
-      S.seed[slot] = seed_at(P.sub_cp + 16 * size_t(S.code[k] & IK_MASK), gc);
+    if (overflow) nc = DMAXC;
+    warp_rank(S.tcode, S.tlb, nc, S.code, S.lb, lane);
+    int subs_before = 0;
+    for (int base = 0; base < nc; base += 32) {
+      const int k = base + lane;
+      const bool is_sub = k < nc && (S.code[k] >> IK_SHIFT) == IK_SUB;
+      const unsigned m = __ballot_sync(FULL, is_sub);
+      const int before = subs_before + __popc(m & ((1u << lane) - 1u));
+      subs_before += __popc(m);
+      if (k >= nc) continue;
+      int slot = -1;
+      if (is_sub && before < MAXSUB) {
+        slot = before;
+        S.seed[slot] = seed_at(P.sub_cp + 16 * size_t(S.code[k] & IK_MASK), gc);
+      }
+      S.cert[k] = 0;
+      S.slot[k] = int8_t(slot);
     }
-    S.cert[k] = 0;
-    S.slot[k] = int8_t(slot);
+    __syncwarp();
+    const WarpCands W{S.code, S.lb, S.cert, S.slot, S.seed, S.net, S.net32, nc, overflow};
+    double vv;
+    int ff;
+    warp_point<false>(P, W, c, gc, live && mine, cut, lane, &vv, &ff);
+    if (mine) v = vv, f = ff;
+    l0 += sg;
   }
-  __syncwarp();
-  const WarpCands W{S.code, S.lb, S.cert, S.slot, S.seed, S.net, S.net32, nc, overflow};
-  double v;
-  int f;
-  warp_point<false>(P, W, c, gc, live, cut, lane, &v, &f);
   Box4 kids[8];
   int nk = 0;
   if (live) {
@@ -236,9 +263,15 @@ struct DecideSmemF {
   SeedF seed[MAXSUB];
   double4 net[16];
   float4 net32[16];
+  float4 res[16 * NRES_D];  // the first NRES_D sub-patches' nets, staged by bulk copies
   int8_t cert[DMAXC];
   int8_t slot[DMAXC];
+  int8_t rslot[DMAXC];
+  uint32_t residx[NRES_D];
+  uint64_t bar;
+  uint32_t phase;  // the barrier's phase (lane 0 keeps it for the warp)
   int n;
+  int err;         // a bulk copy that did not complete in time
 };
 
 __device__ __forceinline__ void decide_group_f(const DecideArgs& a, const Box4* boxes, int64_t n, long long size,
@@ -254,95 +287,127 @@ __device__ __forceinline__ void decide_group_f(const DecideArgs& a, const Box4* 
   const double3 c = (lo + hi) * 0.5;
   const double r = 0.5 * len(hi - lo);
   const double cut = (r + a.clamp) * (1.0 + 1e-4);
-  double bl[3] = {c.x, c.y, c.z}, bh[3] = {c.x, c.y, c.z};
-  for (int o = 16; o > 0; o >>= 1)
-    for (int k = 0; k < 3; k++) {
-      bl[k] = fmin(bl[k], __shfl_xor_sync(FULL, bl[k], o));
-      bh[k] = fmax(bh[k], __shfl_xor_sync(FULL, bh[k], o));
+  const int glanes = int(min(int64_t(gs), n - g0));  // lanes of the group holding a box
+  double v = 0.0, verr = 0.0;
+  int f = 1;
+  for (int l0 = 0, sg = glanes; l0 < glanes;) {
+    sg = min(sg, glanes - l0);
+    const bool mine = lane >= l0 && lane < l0 + sg;
+    const bool mlive = live && mine;
+    double3 gc;
+    double R, bl[3], bh[3];
+    centres_ball(c, mine, l0, lane, &gc, &R, bl, bh);
+    int nc = warp_list<DMAXC>(P, a.leaves, a.n_leaves, gc, R + cut, S.u.list.tcode, S.u.list.tlb, S.u.list.fr, &S.n,
+                              lane);
+    const bool overflow = nc > DMAXC;
+    if (overflow && sg > 1) {
+      sg = (sg + 1) / 2;
+      continue;
     }
-  const double3 gc = mk(0.5 * (bl[0] + bh[0]), 0.5 * (bl[1] + bh[1]), 0.5 * (bl[2] + bh[2]));
-  double R = len(c - gc);
-  for (int o = 16; o > 0; o >>= 1) R = fmax(R, __shfl_xor_sync(FULL, R, o));
-  int nc = warp_list<DMAXC>(P, a.leaves, a.n_leaves, gc, R + cut, S.u.list.tcode, S.u.list.tlb, S.u.list.fr, &S.n,
-                            lane);
-  const bool overflow = nc > DMAXC;
-  if (overflow) nc = DMAXC;
-  warp_rank(S.u.list.tcode, S.u.list.tlb, nc, S.code, S.lb, lane);
-  const double3 blo = mk(bl[0], bl[1], bl[2]), bhi = mk(bh[0], bh[1], bh[2]);
-  int subs_before = 0;
-  for (int base = 0; base < nc; base += 32) {
-    const int k = base + lane;
-    const bool is_sub = k < nc && (S.code[k] >> IK_SHIFT) == IK_SUB;
-    const unsigned m = __ballot_sync(FULL, is_sub);
-    const int before = subs_before + __popc(m & ((1u << lane) - 1u));
-    subs_before += __popc(m);
-    if (k >= nc) continue;
-    const uint32_t code = S.code[k], idx = code & IK_MASK;
-    int slot = -1;
-    int8_t cert = 0;
-    float4 g0v = make_float4(0.f, 0.f, 0.f, 0.f), g1v = g0v;
-    S.lbf[k] = __double2float_rd(S.lb[k]);
-    if (is_sub) {
-      const DSub& s = P.subs[idx];
-      cert = sub_convex(s, blo, bhi) ? 1 : 0;
-      g0v = make_float4(float(s.c[0] - gc.x), float(s.c[1] - gc.y), float(s.c[2] - gc.z), float(P.faces[s.face].sense));
-      g1v = make_float4(__double2float_ru(0.5 * (s.box[3] - s.box[0])), __double2float_ru(0.5 * (s.box[4] - s.box[1])),
-                        __double2float_ru(0.5 * (s.box[5] - s.box[2])), 0.f);
-      if (before < MAXSUB) {
-        slot = before;
-        const float3 qc = f3(float(gc.x - s.c[0]), float(gc.y - s.c[1]), float(gc.z - s.c[2]));
-        S.seed[slot] = seed_at_f(P.sub_cp32 + 16 * size_t(idx), qc, 0.5f, 0.5f);
-      }
-    } else if ((code >> IK_SHIFT) == IK_FACE) {
-      const DFace& f = P.faces[idx];
-      if (f.kind == S_PLANE) {
-        const double3 z = ld3(f.z) * f.sense, o = ld3(f.o);
-        g0v = make_float4(float(z.x), float(z.y), float(z.z), float(dot(o - gc, z)));
-        double tlo[2] = {INFINITY, INFINITY}, thi[2] = {-INFINITY, -INFINITY};
-        const double3 zz = ld3(f.z), fx = ld3(f.x), fy = ld3(f.y);
-        for (int q = 0; q < 8; q++) {
-          double3 x = mk(q & 1 ? bh[0] : bl[0], q & 2 ? bh[1] : bl[1], q & 4 ? bh[2] : bl[2]);
-          double3 e = (x - zz * dot(x - o, zz)) - o;
-          double u = dot(e, fx), v = dot(e, fy);
-          tlo[0] = fmin(tlo[0], u), thi[0] = fmax(thi[0], u);
-          tlo[1] = fmin(tlo[1], v), thi[1] = fmax(thi[1], v);
+    if (overflow) nc = DMAXC;
+    warp_rank(S.u.list.tcode, S.u.list.tlb, nc, S.code, S.lb, lane);
+    const double3 blo = mk(bl[0], bl[1], bl[2]), bhi = mk(bh[0], bh[1], bh[2]);
+    int subs_before = 0;
+    for (int base = 0; base < nc; base += 32) {
+      const int k = base + lane;
+      const bool is_sub = k < nc && (S.code[k] >> IK_SHIFT) == IK_SUB;
+      const unsigned m = __ballot_sync(FULL, is_sub);
+      const int before = subs_before + __popc(m & ((1u << lane) - 1u));
+      subs_before += __popc(m);
+      if (k >= nc) continue;
+      const uint32_t code = S.code[k], idx = code & IK_MASK;
+      int slot = -1, rslot = -1;
+      int8_t cert = 0;
+      float4 g0v = make_float4(0.f, 0.f, 0.f, 0.f), g1v = g0v;
+      S.lbf[k] = __double2float_rd(S.lb[k]);
+      if (is_sub) {
+        const DSub& s = P.subs[idx];
+        cert = sub_convex(s, blo, bhi) ? 1 : 0;
+        g0v = make_float4(float(s.c[0] - gc.x), float(s.c[1] - gc.y), float(s.c[2] - gc.z), float(P.faces[s.face].sense));
+        g1v = make_float4(__double2float_ru(0.5 * (s.box[3] - s.box[0])), __double2float_ru(0.5 * (s.box[4] - s.box[1])),
+                          __double2float_ru(0.5 * (s.box[5] - s.box[2])), s.klass == 1 ? 1.f : 0.f);
+        if (before < NRES_D) {
+          rslot = before;
+          S.residx[before] = idx;
         }
-        double mg = 1e-9 * (1.0 + fmax(fmax(fabs(tlo[0]), fabs(thi[0])), fmax(fabs(tlo[1]), fabs(thi[1]))));
-        tlo[0] -= mg, tlo[1] -= mg, thi[0] += mg, thi[1] += mg;
-        const int cls = trim_box_class(P, f, tlo, thi);
-        cert = cls == 1 ? 1 : (cls == 0 ? 2 : 0);
-      } else {
-        g0v.w = NAN;
+        if (before < MAXSUB) {
+          slot = before;
+          const float3 qc = f3(float(gc.x - s.c[0]), float(gc.y - s.c[1]), float(gc.z - s.c[2]));
+          S.seed[slot] = seed_at_f(P.sub_cp32 + 16 * size_t(idx), qc, 0.5f, 0.5f);
+        }
+      } else if ((code >> IK_SHIFT) == IK_FACE) {
+        const DFace& f = P.faces[idx];
+        if (f.kind == S_PLANE) {
+          const double3 z = ld3(f.z) * f.sense, o = ld3(f.o);
+          g0v = make_float4(float(z.x), float(z.y), float(z.z), float(dot(o - gc, z)));
+          double tlo[2] = {INFINITY, INFINITY}, thi[2] = {-INFINITY, -INFINITY};
+          const double3 zz = ld3(f.z), fx = ld3(f.x), fy = ld3(f.y);
+          for (int q = 0; q < 8; q++) {
+            double3 x = mk(q & 1 ? bh[0] : bl[0], q & 2 ? bh[1] : bl[1], q & 4 ? bh[2] : bl[2]);
+            double3 e = (x - zz * dot(x - o, zz)) - o;
+            double u = dot(e, fx), v = dot(e, fy);
+            tlo[0] = fmin(tlo[0], u), thi[0] = fmax(thi[0], u);
+            tlo[1] = fmin(tlo[1], v), thi[1] = fmax(thi[1], v);
+          }
+          double mg = 1e-9 * (1.0 + fmax(fmax(fabs(tlo[0]), fabs(thi[0])), fmax(fabs(tlo[1]), fabs(thi[1]))));
+          tlo[0] -= mg, tlo[1] -= mg, thi[0] += mg, thi[1] += mg;
+          const int cls = trim_box_class(P, f, tlo, thi);
+          cert = cls == 1 ? 1 : (cls == 0 ? 2 : 0);
+        } else {
+          g0v.w = NAN;
+        }
+      }
+      S.u.geo[2 * k] = g0v;
+      S.u.geo[2 * k + 1] = g1v;
+      S.cert[k] = cert;
+      S.slot[k] = int8_t(slot);
+      S.rslot[k] = int8_t(rslot);
+    }
+    // the first NRES_D sub-patches' nets into shared memory for the group
+    const int nres = min(subs_before, NRES_D);
+    __syncwarp();
+    if (nres > 0) {
+      uint32_t ph = S.phase;
+      if (lane == 0) stage_nets(S.res, P.sub_cp32, S.residx, nres, &S.bar);
+      if (!mbar_wait(&S.bar, ph)) {  // never expected: let the copies land, then read from global
+        mbar_wait(&S.bar, ph);
+        if (lane == 0) S.err = 1;
+      }
+      __syncwarp();
+      if (lane == 0) S.phase = ph ^ 1u;
+    }
+    __syncwarp();
+    float vf = 0.f;
+    int ff = 3;
+    if (!overflow) {
+      int8_t* rs = S.rslot;
+      if (S.err) {  // no resident nets: every net from global memory
+        for (int k = lane; k < nc; k += 32) rs[k] = -1;
+        __syncwarp();
+      }
+      const WarpCandsF W{S.code, S.lbf, S.cert, S.slot, S.seed, S.u.geo, S.net32, S.res, rs, nc, 16};
+      int lastk = -1;
+      float ls = 0.f, lt = 0.f;
+      ff = warp_point_f(P, W, f3(float(c.x - gc.x), float(c.y - gc.y), float(c.z - gc.z)), c, mlive, float(cut),
+                        lane, &vf, &lastk, &ls, &lt);
+    }
+    if (mine) {
+      v = vf, f = ff, verr = 0.0;
+      if (f == 0) {
+        verr = 1e-4 + 4e-6 * (fabs(v) + R);
+        if (fabs(fabs(v) - (r + a.clamp)) <= verr) f = 3;  // the verdict is within the float error
       }
     }
-    S.u.geo[2 * k] = g0v;
-    S.u.geo[2 * k + 1] = g1v;
-    S.cert[k] = cert;
-    S.slot[k] = int8_t(slot);
-  }
-  __syncwarp();
-  float vf = 0.f;
-  int f = 3;
-  if (!overflow) {
-    const WarpCandsF W{S.code, S.lbf, S.cert, S.slot, S.seed, S.u.geo, S.net32, nc};
-    int lastk = -1;
-    float ls = 0.f, lt = 0.f;
-    f = warp_point_f(P, W, f3(float(c.x - gc.x), float(c.y - gc.y), float(c.z - gc.z)), c, live, float(cut), lane,
-                     &vf, &lastk, &ls, &lt);
-  }
-  double v = vf, verr = 0.0;
-  if (f == 0) {
-    verr = 1e-4 + 4e-6 * (fabs(v) + R);
-    if (fabs(fabs(v) - (r + a.clamp)) <= verr) f = 3;  // the verdict is within the float error
-  }
-  const bool pd = live && f == 3;
-  if (__any_sync(FULL, pd)) {  // the double walk over the same candidates, centre starts
-    const WarpCands W64{S.code, S.lb, S.cert, nullptr, nullptr, S.net, S.net32, nc, overflow};
-    double v64;
-    int f64;
-    warp_point<false>(P, W64, c, gc, pd, cut, lane, &v64, &f64);
-    if (pd) v = v64, f = f64, verr = 0.0;
-    if (a.n_double && pd) atomicAdd(a.n_double, 1ull);
+    const bool pd = mlive && f == 3;
+    if (__any_sync(FULL, pd)) {  // the double walk over the same candidates, centre starts
+      const WarpCands W64{S.code, S.lb, S.cert, nullptr, nullptr, S.net, S.net32, nc, overflow};
+      double v64;
+      int f64;
+      warp_point<false>(P, W64, c, gc, pd, cut, lane, &v64, &f64);
+      if (pd) v = v64, f = f64, verr = 0.0;
+      if (a.n_double && pd) atomicAdd(a.n_double, 1ull);
+    }
+    l0 += sg;
   }
   Box4 kids[8];
   int nk = 0;
@@ -460,10 +525,21 @@ __global__ void __launch_bounds__(DWARPS * 32, 2) k_decide_w(DecideArgs a, int g
 
 // The mixed form's decision of one box size: three blocks a SM (the float walk's
 // registers), the groups' room in dynamic shared memory.
-__global__ void __launch_bounds__(DWARPS * 32, 3) k_decide_wf(DecideArgs a, int gs) {
+// A warp's bulk-copy barrier, once at the start of a float decision kernel.
+__device__ __forceinline__ void decide_f_init(DecideSmemF& S, int lane) {
+  if (lane == 0) {
+    mbar_init(&S.bar);
+    S.phase = 0;
+    S.err = 0;
+  }
+  __syncwarp();
+}
+
+__global__ void __launch_bounds__(DWARPS * 32, ICAM_MIXED_BLOCKS) k_decide_wf(DecideArgs a, int gs) {
   extern __shared__ __align__(16) unsigned char dsm[];
   DecideSmemF* smem = reinterpret_cast<DecideSmemF*>(dsm);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  decide_f_init(smem[warp], lane);
   for (int64_t g0 = (int64_t(blockIdx.x) * DWARPS + warp) * gs; g0 < a.n; g0 += int64_t(gridDim.x) * DWARPS * gs)
     decide_group_f(a, a.boxes, a.n, a.size, g0, gs, smem[warp], lane, a.first_sd != nullptr);
 }
@@ -500,9 +576,10 @@ __global__ void k_decide_prep(DecideBatchArgs b, int round) {
 // A batch's round: every part's boxes of this round's size, 32 of one part a warp, the
 // warps taking groups across all parts from the numbering k_decide_prep made.
 template <bool F32>
-__global__ void __launch_bounds__(DWARPS * 32, F32 ? 3 : 2) k_decide_batch(DecideBatchArgs b, int round) {
+__global__ void __launch_bounds__(DWARPS * 32, F32 ? ICAM_MIXED_BLOCKS : 2) k_decide_batch(DecideBatchArgs b, int round) {
   extern __shared__ __align__(16) unsigned char dsm[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (F32) decide_f_init(reinterpret_cast<DecideSmemF*>(dsm)[warp], lane);
   const int64_t total = b.groups[b.n_parts];
   const int gs = int(b.groups[b.n_parts + 1]);
   for (int64_t g = int64_t(blockIdx.x) * DWARPS + warp; g < total; g += int64_t(gridDim.x) * DWARPS) {
@@ -532,7 +609,7 @@ __global__ void __launch_bounds__(256) k_first_signs_batch(DecideBatchArgs b) {
 void launch_decide(const DecideArgs& a, cudaStream_t s, bool first, bool mixed) {
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int per_sm = mixed ? 3 : 2;
+  const int per_sm = mixed ? ICAM_MIXED_BLOCKS : 2;
   const int gs = group_size(a.n, sms);
   const int64_t want = (a.n + DWARPS * gs - 1) / (DWARPS * gs);
   const int grid = int(std::max<int64_t>(1, std::min<int64_t>(want, int64_t(sms) * per_sm)));
@@ -556,7 +633,7 @@ void launch_decide_batch(const DecideBatchArgs& b, int rounds, cudaStream_t s) {
   for (int r = 0; r < rounds; r++) {
     k_decide_prep<<<1, 32, 0, s>>>(bb, r);
     if (b.mixed)
-      k_decide_batch<true><<<sms * 3, DWARPS * 32, smem, s>>>(bb, r);
+      k_decide_batch<true><<<sms * ICAM_MIXED_BLOCKS, DWARPS * 32, smem, s>>>(bb, r);
     else
       k_decide_batch<false><<<sms * 2, DWARPS * 32, smem, s>>>(bb, r);
     if (r == 0) k_first_signs_batch<<<b.n_parts, 256, 0, s>>>(bb);

@@ -11,6 +11,14 @@
 
 namespace icam {
 
+// Blocks of four warps a SM for the mixed form's kernels: the register budget their
+// launch bounds give (65536 / (ICAM_MIXED_BLOCKS x 128) a thread). Measured on the
+// freeform level at h = 0.1 mm: two blocks (255 registers) 36.8 ms a bake, three (168
+// registers, the out-of-line double paths spilling past L1) 40.9 ms.
+#ifndef ICAM_MIXED_BLOCKS
+#define ICAM_MIXED_BLOCKS 2
+#endif
+
 // A float distance below this (mm) leaves its sign to the double walk: the float
 // answers' error is ~1e-6 mm on the rebased nets, so above it the sign is sure.
 constexpr float NEAR_ZERO = 1e-4f;
@@ -83,11 +91,53 @@ static __device__ __noinline__ bool rare_item_cold(const DPack& P, uint32_t code
   return true;
 }
 
+// Control nets a warp keeps in shared memory for a whole brick (or box group): the
+// first NRES sub-patches of its ranked list, staged by the tensor memory accelerator's
+// bulk copies (cp.async.bulk, global to shared, completion on an mbarrier).
+constexpr int NRES = 12;  // brick kernel; the box decision keeps NRES_D
+constexpr int NRES_D = 8;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return uint32_t(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// Lane 0: the bulk copies of n float nets (sub-patches idx[k], 256 bytes each, from
+// cp32) into dst + 16 k, completing on the warp's barrier. Source and destination are
+// 16-byte aligned (nets of 16 float4), as the bulk copy requires.
+__device__ __forceinline__ void stage_nets(float4* dst, const float4* cp32, const uint32_t* idx, int n,
+                                           uint64_t* bar) {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // after the generic reads of the room
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(uint32_t(n) * 256u) : "memory");
+  for (int k = 0; k < n; k++)
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], 256, [%2];" ::"r"(
+                     smem_u32(dst + 16 * k)),
+                 "l"(cp32 + 16 * size_t(idx[k])), "r"(smem_u32(bar))
+                 : "memory");
+}
+// Every lane: waits for the barrier's phase `parity` to complete, at most `limit` tries;
+// false when it gave up.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int limit = 1 << 22) {
+  for (int i = 0; i < limit; i++) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
 // A warp's ranked candidates for the float walk, in shared memory: code, bound at the
-// centre rounded down, verdict (as WarpCands), seed slot, and two float4 of geometry
-// relative to the centre c: a plane (z * sense, (o - c).(z * sense)), (NaN: a curved
-// face); a sub-patch (its rebasing origin - c, the face's sense), (its control box's
-// half extents).
+// centre rounded down, verdict (as WarpCands), seed slot, resident net slot (-1: load
+// it), and two float4 of geometry relative to the centre c: a plane (z * sense,
+// (o - c).(z * sense)), (NaN: a curved face); a sub-patch (its rebasing origin - c, the
+// face's sense), (its control box's half extents, 1 if wholly inside its face's loops).
 struct WarpCandsF {
   const uint32_t* code;
   const float* lb;
@@ -95,8 +145,11 @@ struct WarpCandsF {
   const int8_t* slot;
   const SeedF* seed;
   const float4* geo;
-  float4* net32;
+  float4* net32;       // the room for a net not resident
+  const float4* res;   // the resident nets, 16 float4 each
+  const int8_t* rslot;
   int n;
+  int iters;           // float Newton iterations a solve
 };
 
 // The float walk of the lane's node (pc: its offset from the centre; p: the node in
@@ -119,15 +172,26 @@ __device__ __forceinline__ int warp_point_f(const DPack& P, const WarpCandsF& W,
   bool pend = false;
   int wk = -1;
   float ws = 0.f, wt = 0.f;
+  // sub-patches whose certificate fails here: left for the double subdivision once
+  // everything else has tightened the bound (the first two; more: the double walk)
+  uint32_t dc0 = 0, dc1 = 0;
+  float dl0 = 0.f, dl1 = 0.f, und = INFINITY;
+  int nd = 0;
   for (int k = 0; k < W.n; k++) {
     const float lbc = W.lb[k];
     if (__all_sync(FULL, lbc - rr >= best)) break;  // ranked: nothing later is nearer
     const uint32_t code = W.code[k];
     const uint32_t kind = code >> IK_SHIFT, idx = code & IK_MASK;
-    if (kind == IK_SUB) {  // the float net to shared memory, by the whole warp
-      __syncwarp();
-      if (lane < 16) W.net32[lane] = P.sub_cp32[16 * size_t(idx) + lane];
-      __syncwarp();
+    const float4* net = W.net32;
+    if (kind == IK_SUB) {
+      const int rs = W.rslot[k];
+      if (rs >= 0) {
+        net = W.res + 16 * rs;
+      } else {  // not resident: to shared memory by the whole warp
+        __syncwarp();
+        if (lane < 16) W.net32[lane] = P.sub_cp32[16 * size_t(idx) + lane];
+        __syncwarp();
+      }
     }
     if (lbc - rr >= best) continue;
     const float4 g0 = W.geo[2 * k];
@@ -148,11 +212,15 @@ __device__ __forceinline__ int warp_point_f(const DPack& P, const WarpCandsF& W,
       const float3 q = f3(pc.x - g0.x, pc.y - g0.y, pc.z - g0.z);
       const float bx = fmaxf(fabsf(q.x) - g1.x, 0.f), by = fmaxf(fabsf(q.y) - g1.y, 0.f),
                   bz = fmaxf(fabsf(q.z) - g1.z, 0.f);
-      if (!(sqrtf(bx * bx + by * by + bz * bz) < best)) continue;
-      const DSub& s = P.subs[idx];
-      if (!W.cert[k] && !sub_convex_at(s, p)) {  // the double walk searches it by subdivision
-        pend = true;
-        best = -1.f;
+      const float blb = sqrtf(bx * bx + by * by + bz * bz);
+      if (!(blb < best)) continue;
+      if (!W.cert[k] && !sub_convex_at(P.subs[idx], p)) {  // subdivision, after the rest
+        und = fminf(und, blb);
+        if (nd == 0)
+          dc0 = code, dl0 = blb;
+        else if (nd == 1)
+          dc1 = code, dl1 = blb;
+        nd++;
         continue;
       }
       float sf = 0.5f, tf = 0.5f;
@@ -162,7 +230,7 @@ __device__ __forceinline__ int warp_point_f(const DPack& P, const WarpCandsF& W,
         seed_params_f(W.seed[W.slot[k]], pc, &sf, &tf);
       }
       SEf ef;
-      if (!newton_bicubic_f(W.net32, q, &sf, &tf, 8, &ef)) {  // stalled: the double walk
+      if (!newton_bicubic_f(net, q, &sf, &tf, W.iters, &ef)) {  // stalled: the double walk
         pend = true;
         best = -1.f;
         continue;
@@ -173,8 +241,11 @@ __device__ __forceinline__ int warp_point_f(const DPack& P, const WarpCandsF& W,
       const float3 nf = f3(ef.ps.y * ef.pt.z - ef.ps.z * ef.pt.y, ef.ps.z * ef.pt.x - ef.ps.x * ef.pt.z,
                            ef.ps.x * ef.pt.y - ef.ps.y * ef.pt.x);
       if (!(dotf(nf, nf) > 0.f)) continue;
-      if (s.klass != 1 && !trim_at_cold(P, s.face, s.u0 + double(sf) * (s.u1 - s.u0), s.v0 + double(tf) * (s.v1 - s.v0)))
-        continue;
+      if (g1.w != 1.f) {  // across its face's loops: the trim test in double
+        const DSub& s = P.subs[idx];
+        if (!trim_at_cold(P, s.face, s.u0 + double(sf) * (s.u1 - s.u0), s.v0 + double(tf) * (s.v1 - s.v0)))
+          continue;
+      }
       best = d32;
       sdv = -dotf(rf, nf) * g0.w < 0.f ? -d32 : d32;
       wk = k, ws = sf, wt = tf;
@@ -188,6 +259,20 @@ __device__ __forceinline__ int warp_point_f(const DPack& P, const WarpCandsF& W,
   }
   if (!live) return 1;
   if (wk >= 0) *lastk = wk, *ls = ws, *lt = wt;
+  if (!pend && nd > 0 && und < best) {  // the deferred sub-patches, by the double subdivision
+    if (nd > 2) {
+      pend = true;
+    } else {
+      double b64 = best, s64 = sdv, u64 = INFINITY;
+      point_resolve(P, p, dc0, dl0, dc1, dl1, nd, &b64, &s64, &u64);
+      if (u64 < b64) {
+        pend = true;
+      } else if (b64 < double(best)) {
+        best = float(b64), sdv = float(s64);
+        wk = -1;
+      }
+    }
+  }
   if (pend) return 3;
   if (!isnan(sdv) && best <= capw) {
     if (best < NEAR_ZERO && !(best < qzero)) return 3;  // the sign near zero: double precision decides it

@@ -141,7 +141,10 @@ class PartGpu:
             self.h = None
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except TypeError:  # interpreter shutdown: the module's globals are gone
+            pass
 
     def _check(self, rc, what):
         if rc != 0:
