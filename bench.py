@@ -79,6 +79,16 @@ def workload(seed: int, kind: str = "freeform"):
     return b, lo, nb
 
 
+def newton_figures(st):
+    """The mixed forms' in-bake Newton work from a bake's stats: solves of sub-patches
+    at the nodes, evaluations a solve (its iterations), nodes and box centres read again
+    in double precision."""
+    solves = st.get("newton_solves", 0)
+    return {"newton_solves": solves,
+            "newton_iters_per_solve": st.get("newton_evals", 0) / solves if solves else None,
+            "nodes_double": st.get("nodes_double", 0), "centres_double": st.get("centres_double", 0)}
+
+
 def over_ranks(dist, device, ms, voxels=None):
     """The job's figures over the ranks: the slowest rank's time (max) and every rank's
     voxels (sum); as given on one process. Every rank calls it at the same point."""
@@ -318,7 +328,8 @@ def main():
         others[name] = {"value": o_vox * args.steps / (o_ms * 1e-3), "ms_per_step": o_ms / args.steps,
                         "stage_ms": {"decide": float(np.mean([x["ms_decide"] for x in o_stats])),
                                      "nodes": float(np.mean([x["ms_nodes"] for x in o_stats])),
-                                     "assemble": float(np.mean([x["ms_post"] for x in o_stats]))}}
+                                     "assemble": float(np.mean([x["ms_post"] for x in o_stats]))},
+                        **newton_figures(o_stats[-1])}
     if smi:
         smi.terminate()
         smi.wait()
@@ -375,7 +386,7 @@ def main():
             "bricks_read": st["bricks_read"], "bricks_stored": st["bricks_words"],
             "bricks_settled": st["bricks_settled"],
             "nodes_exact": st["nodes_exact"], "nodes_undecided": st["nodes_undecided"],
-            "nodes_double": st["nodes_double"], "centres_double": st["centres_double"],
+            **newton_figures(st),
             "nodes_exact_per_s": st["nodes_exact"] * args.steps / (total_ms * 1e-3),
             "stage_ms": {"decide": st["ms_decide"], "nodes": st["ms_nodes"], "assemble": st["ms_post"]},
             "gpu_launches": int(st["kernel_launches"]) * args.steps,

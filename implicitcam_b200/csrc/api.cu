@@ -140,7 +140,7 @@ int icam_pack_create(const IcamSolidDesc* solid, const IcamPackOptions* opt, Ica
   u |= upload(pk, pk->leaves_host, &lv);
   pk->leaves = const_cast<int32_t*>(lv);
   void* st = nullptr;
-  if (cudaMalloc(&st, 16 * sizeof(unsigned long long)) == cudaSuccess) {
+  if (cudaMalloc(&st, kStatCount * sizeof(unsigned long long)) == cudaSuccess) {
     pk->owned.push_back(st);
     pk->d_stats = static_cast<unsigned long long*>(st);
   } else {
@@ -250,12 +250,12 @@ int icam_bricks(IcamPack* pk, const double* first_nodes, size_t n, double h, dou
   a.d_out = (double*)dval;
   a.flag_out = (int8_t*)dflag;
   a.stats = pk->d_stats;
-  CK(cudaMemsetAsync(pk->d_stats, 0, 16 * sizeof(unsigned long long), pk->stream));
+  CK(cudaMemsetAsync(pk->d_stats, 0, kStatCount * sizeof(unsigned long long), pk->stream));
   launch_bricks(a, pk->stream);
   CK(cudaGetLastError());
   std::vector<double> v(n * 729);
   std::vector<int8_t> f(n * 729);
-  unsigned long long st[16];
+  unsigned long long st[kStatCount];
   CK(cudaMemcpyAsync(v.data(), dval, n * 729 * sizeof(double), cudaMemcpyDeviceToHost, pk->stream));
   CK(cudaMemcpyAsync(f.data(), dflag, n * 729, cudaMemcpyDeviceToHost, pk->stream));
   CK(cudaMemcpyAsync(st, pk->d_stats, sizeof(st), cudaMemcpyDeviceToHost, pk->stream));
@@ -444,7 +444,7 @@ static int bake_level(IcamPack* pk, double h, const double lo[3], const int64_t 
   cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, (int64_t*)nullptr, (int64_t*)nullptr, R + 1, s);
   const size_t Rb = size_t(std::max<int64_t>(R, 1));
   if ((r = scratch(pk, 11, tmp_bytes + 16, &d_tmp)) || (r = scratch(pk, 12, Rb * 3 * sizeof(double), &d_first)) ||
-      (r = scratch(pk, 13, Rb * 365 * sizeof(uint32_t), &d_words)) || (r = scratch(pk, 14, Rb * sizeof(int32_t), &d_kind)) ||
+      (r = scratch(pk, 13, Rb * WORD_STRIDE * sizeof(uint32_t), &d_words)) || (r = scratch(pk, 14, Rb * sizeof(int32_t), &d_kind)) ||
       (r = scratch(pk, 15, (Rb + 1) * 2 * sizeof(int64_t), &d_flag)))
     return r;
   d_slot = (int64_t*)d_flag + (Rb + 1);
@@ -471,7 +471,7 @@ static int bake_level(IcamPack* pk, double h, const double lo[3], const int64_t 
     b.words_out = (uint32_t*)d_words;
     b.kind_out = (int32_t*)d_kind;
     b.stats = pk->d_stats;
-    CK(cudaMemsetAsync(pk->d_stats, 0, 16 * sizeof(unsigned long long), s));
+    CK(cudaMemsetAsync(pk->d_stats, 0, kStatCount * sizeof(unsigned long long), s));
     launch_bricks(b, s);
     launches++;
     CK(cudaGetLastError());
@@ -504,7 +504,7 @@ static int bake_level(IcamPack* pk, double h, const double lo[3], const int64_t 
   pk->last_atlas = (const uint32_t*)d_atlas;
   pk->last_map_entries = size_t(nb[0] * nb[1] * nb[2]);
   pk->last_slots = nwords_slots;
-  unsigned long long st[16] = {0};
+  unsigned long long st[kStatCount] = {0};
   if (R > 0) CK(cudaMemcpy(st, pk->d_stats, sizeof(st), cudaMemcpyDeviceToHost));
   if (st[13]) {
     for (auto& e : ev) cudaEventDestroy(e);
@@ -524,6 +524,8 @@ static int bake_level(IcamPack* pk, double h, const double lo[3], const int64_t 
     stats->kernel_launches = launches;
     stats->nodes_double = R ? int64_t(st[12]) : 0;
     stats->centres_double = D.centres_double;
+    stats->newton_solves = R ? int64_t(st[17]) : 0;
+    stats->newton_evals = R ? int64_t(st[16]) : 0;
     stats->h2d_bytes = D.h2d_bytes;
     stats->d2h_bytes = D.d2h_bytes + int64_t(sizeof(st));
     float ms;
@@ -751,12 +753,13 @@ int icam_warm(IcamPack* pk, double secs) {
 
 namespace {
 
-constexpr size_t kStaticStats = 0;  // 16 counters of the brick kernel
+constexpr size_t kStaticStats = 0;  // the brick kernel's kStatCount counters
 constexpr size_t kStaticFirst = 256;
 constexpr size_t kStaticD = kStaticFirst + size_t(ICAM_STATIC_BRICKS) * 3 * sizeof(double);
 constexpr size_t kStaticPairs = kStaticD + size_t(ICAM_STATIC_BRICKS) * ICAM_NODES * sizeof(double);
 constexpr size_t kStaticFlag = kStaticPairs + size_t(ICAM_STATIC_BRICKS) * ICAM_NODES * 2 * sizeof(float);
 constexpr size_t kStaticBytes = kStaticFlag + size_t(ICAM_STATIC_BRICKS) * ICAM_NODES;
+static_assert(kStatCount * sizeof(unsigned long long) <= kStaticFirst, "the counters fit before the first nodes");
 static_assert(kStaticFirst % 256 == 0 && kStaticD % 256 == 0 && kStaticPairs % 256 == 0 && kStaticFlag % 256 == 0,
               "static scratch regions are 256-byte aligned");
 
@@ -818,7 +821,7 @@ extern "C" int icam_bricks_static(IcamPack* pk, const double* first_nodes, size_
   auto* dflag = reinterpret_cast<int8_t*>(base + kStaticFlag);
   const int64_t m = int64_t(n) * ICAM_NODES;
   SCK(cudaMemcpyAsync(dfirst, first_nodes, n * 3 * sizeof(double), cudaMemcpyHostToDevice, pk->stream));
-  SCK(cudaMemsetAsync(stats, 0, 16 * sizeof(unsigned long long), pk->stream));
+  SCK(cudaMemsetAsync(stats, 0, kStatCount * sizeof(unsigned long long), pk->stream));
   BrickArgs a{};
   a.P = pk->dev;
   a.firsts = dfirst;

@@ -80,7 +80,7 @@ __global__ void k_assemble_batch(const int64_t* idx, const int32_t* part_of, con
       maps[part][idx[i]] = k == 1 ? 0xffffffffu : (k == 2 ? 0xfffffffeu : uint32_t(local));
     }
     if (k == 0)
-      for (int w = threadIdx.x; w < 365; w += blockDim.x) atlas[slot[i] * 365 + w] = words[i * 365 + w];
+      for (int w = threadIdx.x; w < 365; w += blockDim.x) atlas[slot[i] * 365 + w] = words[i * WORD_STRIDE + w];
   }
 }
 
@@ -173,7 +173,7 @@ int icam_batch_create(IcamPack* const* packs, size_t n, IcamBatch** out, char* e
   if (cudaMalloc(&p, n * sizeof(PartParams)) != cudaSuccess) return done(ICAM_ERR_CUDA, "cudaMalloc");
   bt->owned.push_back(p);
   bt->d_parts = static_cast<PartParams*>(p);
-  if (cudaMalloc(&p, 16 * sizeof(unsigned long long)) != cudaSuccess) return done(ICAM_ERR_CUDA, "cudaMalloc");
+  if (cudaMalloc(&p, kStatCount * sizeof(unsigned long long)) != cudaSuccess) return done(ICAM_ERR_CUDA, "cudaMalloc");
   bt->owned.push_back(p);
   bt->d_stats = static_cast<unsigned long long*>(p);
   return done(ICAM_OK, "");
@@ -352,7 +352,7 @@ int icam_batch_bake(IcamBatch* bt, const IcamBatchLevel* levels, int precision, 
                                   (double*)nullptr, R, 0, end_bit, s);
   if ((r = bbuf(bt, 0, Rb * 3 * sizeof(double), &firsts)) || (r = bbuf(bt, 1, Rb * sizeof(double), &dcs)) ||
       (r = bbuf(bt, 2, Rb * sizeof(int64_t), &idx)) || (r = bbuf(bt, 3, Rb * sizeof(int32_t), &part_of)) ||
-      (r = bbuf(bt, 4, Rb * 365 * sizeof(uint32_t), &words)) || (r = bbuf(bt, 5, Rb * sizeof(int32_t), &kind)) ||
+      (r = bbuf(bt, 4, Rb * WORD_STRIDE * sizeof(uint32_t), &words)) || (r = bbuf(bt, 5, Rb * sizeof(int32_t), &kind)) ||
       (r = bbuf(bt, 6, (Rb + 1) * 2 * sizeof(int64_t), &flags)) || (r = bbuf(bt, 7, tmp_bytes + 16, &tmp)) ||
       (r = bbuf(bt, 8, Rb * 365 * sizeof(uint32_t), &atlas)) || (r = bbuf(bt, 9, (n + 1) * sizeof(int64_t), &d_off)) ||
       (r = bbuf(bt, 10, n * sizeof(uint32_t*), &d_maps)) || (r = bbuf(bt, 11, (n + 1) * sizeof(int64_t), &d_pslot)) ||
@@ -416,7 +416,7 @@ int icam_batch_bake(IcamBatch* bt, const IcamBatchLevel* levels, int precision, 
     t.n = std::min<int64_t>(R, 65536);
     float best = 1e30f;
     for (int c = 0; c < 3; c++) {
-      BCK(cudaMemsetAsync(bt->d_stats, 0, 16 * sizeof(unsigned long long), s));
+      BCK(cudaMemsetAsync(bt->d_stats, 0, kStatCount * sizeof(unsigned long long), s));
       BCK(cudaEventRecord(ev[2], s));
       launch_bricks(t, s, choices[c]);
       BCK(cudaGetLastError());
@@ -440,7 +440,7 @@ int icam_batch_bake(IcamBatch* bt, const IcamBatchLevel* levels, int precision, 
       bt->exec = nullptr;
       cudaGraph_t graph = nullptr;
       BCK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-      cudaMemsetAsync(bt->d_stats, 0, 16 * sizeof(unsigned long long), s);
+      cudaMemsetAsync(bt->d_stats, 0, kStatCount * sizeof(unsigned long long), s);
       launch_bricks(a, s, bt->warps);
       k_is_words<<<grid_of(R, 256), 256, 0, s>>>(static_cast<const int32_t*>(kind), R, static_cast<int64_t*>(flags));
       cudaMemsetAsync(static_cast<int64_t*>(flags) + R, 0, sizeof(int64_t), s);
@@ -467,7 +467,7 @@ int icam_batch_bake(IcamBatch* bt, const IcamBatchLevel* levels, int precision, 
   BCK(cudaEventRecord(ev[3], s));
   std::vector<int64_t> pslot(n + 1, 0);
   if (R > 0) BCK(cudaMemcpyAsync(pslot.data(), d_pslot, (n + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-  unsigned long long st[16] = {0};
+  unsigned long long st[kStatCount] = {0};
   BCK(cudaMemcpyAsync(st, bt->d_stats, sizeof(st), cudaMemcpyDeviceToHost, s));
   BCK(cudaStreamSynchronize(s));
   for (int i = 0; i < n; i++) {

@@ -202,20 +202,28 @@ __device__ int brick_post(T* f, const int8_t* flag, RowMasks& M, double3 first, 
       provisional++;
     }
   __syncwarp();
-  // ---- quantise and pack
+  // ---- quantise and pack: a lane eight nodes, four words stored at once (words is
+  // 16-byte aligned, WORD_STRIDE words a brick; the three past the 365th are zero)
   bool pos = true, nonpos = true;
-  for (int w = lane; w < 365; w += 32) {
-    double q0 = round(fmin(fmax(double(f[2 * w]) / clamp, -1.0), 1.0) * 32767.0);
-    pos = pos && q0 > 0;
-    nonpos = nonpos && q0 <= 0;
-    uint32_t word = uint32_t(uint16_t(int16_t(q0)));
-    if (2 * w + 1 < 729) {
-      double q1 = round(fmin(fmax(double(f[2 * w + 1]) / clamp, -1.0), 1.0) * 32767.0);
-      pos = pos && q1 > 0;
-      nonpos = nonpos && q1 <= 0;
-      word |= uint32_t(uint16_t(int16_t(q1))) << 16;
+  for (int w4 = lane; w4 < 92; w4 += 32) {
+    uint32_t word[4];
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      const int w = 4 * w4 + e;
+      word[e] = 0u;
+      if (w >= 365) continue;
+      double q0 = round(fmin(fmax(double(f[2 * w]) / clamp, -1.0), 1.0) * 32767.0);
+      pos = pos && q0 > 0;
+      nonpos = nonpos && q0 <= 0;
+      word[e] = uint32_t(uint16_t(int16_t(q0)));
+      if (2 * w + 1 < 729) {
+        double q1 = round(fmin(fmax(double(f[2 * w + 1]) / clamp, -1.0), 1.0) * 32767.0);
+        pos = pos && q1 > 0;
+        nonpos = nonpos && q1 <= 0;
+        word[e] |= uint32_t(uint16_t(int16_t(q1))) << 16;
+      }
     }
-    if (words) words[w] = word;
+    if (words) reinterpret_cast<uint4*>(words)[w4] = make_uint4(word[0], word[1], word[2], word[3]);
   }
   const bool all_pos = __all_sync(FULL, pos), all_nonpos = __all_sync(FULL, nonpos);
   if (kind && lane == 0) *kind = all_pos ? 1 : (all_nonpos ? 2 : 0);

@@ -95,7 +95,10 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 2) k_bricks_t(BrickArgs a) {
       }
       const uint32_t q = dc > 0 ? 32767u : uint32_t(uint16_t(int16_t(-32767)));
       if (a.words_out)
-        for (int w = lane; w < 365; w += 32) a.words_out[bi * 365 + w] = w < 364 ? q | (q << 16) : q;
+        for (int w = lane; w < WORD_STRIDE / 4; w += 32)
+          reinterpret_cast<uint4*>(a.words_out + bi * WORD_STRIDE)[w] =
+              w < 91 ? make_uint4(q | (q << 16), q | (q << 16), q | (q << 16), q | (q << 16))
+                     : make_uint4(q, 0u, 0u, 0u);  // word 364 (node 728 alone), then padding
       if (lane == 0) {
         if (a.kind_out) a.kind_out[bi] = dc > 0 ? 1 : 2;
         if (a.stats) atomicAdd(&a.stats[1], 729ull);
@@ -182,7 +185,7 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 2) k_bricks_t(BrickArgs a) {
     // ---- 3. every node: the warp's lanes walk the same ranked candidates together
     int cnt[3] = {0, 0, 0};
     int pending = 0;
-    const WarpCands W{S.code, S.lb, S.cert, S.slot, S.v.seed, S.net, S.net32, n, overflow};
+    const WarpCands W{S.code, S.lb, nullptr, S.cert, S.slot, S.v.seed, S.net, S.net32, n, overflow};
     for (int nn0 = 0; nn0 < 729; nn0 += 32) {
       const int nn = nn0 + lane;
       const bool live = nn < 729;
@@ -225,7 +228,7 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 2) k_bricks_t(BrickArgs a) {
     int provisional = 0;
     if (a.words_out || a.kind_out)
       provisional = brick_post<double>(S.u.f, S.flag, S.v.mk, first, h, clamp, dc, 0.0, n_far,
-                                       a.words_out ? a.words_out + bi * 365 : nullptr,
+                                       a.words_out ? a.words_out + bi * WORD_STRIDE : nullptr,
                                        a.kind_out ? a.kind_out + bi : nullptr, lane);
     if (a.stats) brick_census(P, S.code, n, overflow, n_exact, n_far, n_und, provisional, a.stats, lane);
     __syncwarp();

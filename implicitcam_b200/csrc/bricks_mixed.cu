@@ -34,7 +34,8 @@ struct BrickSmemF {
     unsigned char net[SN_ROOM];  // the seed network's activations, before the nets come
   } x;
   double lb64[MAXC];  // ranked candidates: lower bound at the centre (double, then float
-  float lbf[MAXC];    //   rounded down), code, float geometry (WarpCandsF)
+  float lbf[MAXC];    //   rounded down), the least bound from each on, code, float geometry
+  float lbs[MAXC];    //   (WarpCandsF); lbs holds the ranking keys until the walk
   uint32_t code[MAXC];
   float4 geo[2 * MAXC];
   double4 net[16];  // the control net the double walk is on
@@ -115,7 +116,10 @@ __global__ void __launch_bounds__(MW * 32, ICAM_MIXED_BLOCKS) k_bricks_m(BrickAr
       }
       const uint32_t q = dc > 0 ? 32767u : uint32_t(uint16_t(int16_t(-32767)));
       if (a.words_out)
-        for (int w = lane; w < 365; w += 32) a.words_out[bi * 365 + w] = w < 364 ? q | (q << 16) : q;
+        for (int w = lane; w < WORD_STRIDE / 4; w += 32)
+          reinterpret_cast<uint4*>(a.words_out + bi * WORD_STRIDE)[w] =
+              w < 91 ? make_uint4(q | (q << 16), q | (q << 16), q | (q << 16), q | (q << 16))
+                     : make_uint4(q, 0u, 0u, 0u);  // word 364 (node 728 alone), then padding
       if (lane == 0) {
         if (a.kind_out) a.kind_out[bi] = dc > 0 ? 1 : 2;
         if (a.stats) atomicAdd(&a.stats[1], 729ull);
@@ -154,6 +158,8 @@ __global__ void __launch_bounds__(MW * 32, ICAM_MIXED_BLOCKS) k_bricks_m(BrickAr
           __nv_bfloat16* act = reinterpret_cast<__nv_bfloat16*>(S.x.net);
           sn_forward_warp(net_w, act, reinterpret_cast<float*>(act + 32 * SN_KS), x, y, lane);
           s0 = fminf(fmaxf(y[0], 0.f), 1.f), t0 = fminf(fmaxf(y[1], 0.f), 1.f);
+          // the net's distance from the centre (its third output is d / L), the ranking key
+          if (is_sub) S.lbs[k] = fmaxf(y[2] / net_feat[size_t(S.code[k] & IK_MASK) * SN_FEAT + 12], 0.f);
         }
         if (k >= n) continue;
         const uint32_t code = S.code[k], idx = code & IK_MASK;
@@ -161,6 +167,8 @@ __global__ void __launch_bounds__(MW * 32, ICAM_MIXED_BLOCKS) k_bricks_m(BrickAr
         int8_t cert = 0;
         float4 g0 = make_float4(0.f, 0.f, 0.f, 0.f), g1 = g0;
         S.lbf[k] = __double2float_rd(S.lb64[k]);
+        // the key: the net's distance for a sub-patch it saw (no nearer than the bound), else the bound
+        S.lbs[k] = (net_w && is_sub && before < MAXSUB && !__isnanf(S.lbs[k])) ? fmaxf(S.lbs[k], S.lbf[k]) : S.lbf[k];
         if (is_sub) {
           const DSub& s = P.subs[idx];
           cert = sub_convex(s, first, first + mk(8 * h, 8 * h, 8 * h)) ? 1 : 0;
@@ -206,9 +214,66 @@ __global__ void __launch_bounds__(MW * 32, ICAM_MIXED_BLOCKS) k_bricks_m(BrickAr
         S.slot[k] = int8_t(slot);
         S.rslot[k] = int8_t(rslot);
       }
+      __syncwarp();
+      // ICAM_MIXED_LEARNED: the candidates ranked by the seed network's distance instead of
+      // their bound, so that the walk meets the nearest sub-patch first and the bound it
+      // sets rules the others out; the walk leaves once the least bound of what is left
+      // (lbs, the suffix minimum) is past every lane's answer, so the answers are the same
+      if (net_w) {
+        int pos[MAXC / 32];
+#pragma unroll
+        for (int q = 0; q < MAXC / 32; q++) {
+          const int k = lane + 32 * q;
+          pos[q] = k;
+          if (k < n) {
+            const float key = S.lbs[k];
+            int p = 0;
+            for (int j = 0; j < n; j++) {
+              const float kj = S.lbs[j];
+              p += (kj < key) || (kj == key && j < k);
+            }
+            pos[q] = p;
+          }
+        }
+        auto move = [&](auto* arr) {
+          decltype(+arr[0]) val[MAXC / 32];
+#pragma unroll
+          for (int q = 0; q < MAXC / 32; q++)
+            if (lane + 32 * q < n) val[q] = arr[lane + 32 * q];
+          __syncwarp();
+#pragma unroll
+          for (int q = 0; q < MAXC / 32; q++)
+            if (lane + 32 * q < n) arr[pos[q]] = val[q];
+          __syncwarp();
+        };
+        move(S.code);
+        move(S.lb64);
+        move(S.lbf);
+        move(S.cert);
+        move(S.slot);
+        move(S.rslot);
+        {
+          float4 va[MAXC / 32], vb[MAXC / 32];
+#pragma unroll
+          for (int q = 0; q < MAXC / 32; q++)
+            if (lane + 32 * q < n) va[q] = S.geo[2 * (lane + 32 * q)], vb[q] = S.geo[2 * (lane + 32 * q) + 1];
+          __syncwarp();
+#pragma unroll
+          for (int q = 0; q < MAXC / 32; q++)
+            if (lane + 32 * q < n) S.geo[2 * pos[q]] = va[q], S.geo[2 * pos[q] + 1] = vb[q];
+          __syncwarp();
+        }
+        if (lane == 0) {
+          float m = INFINITY;
+          for (int k = n - 1; k >= 0; k--) {
+            m = fminf(m, S.lbf[k]);
+            S.lbs[k] = m;
+          }
+        }
+        __syncwarp();
+      }
       // the first NRES sub-patches' nets staged into shared memory for the whole brick
       const int nres = min(subs_before, NRES);
-      __syncwarp();
       if (nres > 0) {
         if (lane == 0) stage_nets(S.x.w.res, P.sub_cp32, S.residx, nres, &S.bar);
         if (!mbar_wait(&S.bar, phase)) {  // never expected: record it, let the copies land, leave
@@ -222,9 +287,9 @@ __global__ void __launch_bounds__(MW * 32, ICAM_MIXED_BLOCKS) k_bricks_m(BrickAr
     __syncwarp();
     // ---- 3. the float walk: column 32 g + lane of the 81, swept in z
     int cnt[3] = {0, 0, 0};
-    int pending = 0;
+    int pending = 0, n_evals = 0, n_solves = 0;
     {
-      const WarpCandsF W{S.code, S.lbf, S.cert, S.slot, S.v.seed, S.geo, S.net32, S.x.w.res, S.rslot, n, 8};
+      const WarpCandsF W{S.code, S.lbf, S.lbs, S.cert, S.slot, S.v.seed, S.geo, S.net32, S.x.w.res, S.rslot, n, 8};
       int lastk = -1;
       float ls = 0.f, lt = 0.f;
       const float hf = float(h);
@@ -238,7 +303,8 @@ __global__ void __launch_bounds__(MW * 32, ICAM_MIXED_BLOCKS) k_bricks_m(BrickAr
         const double3 p = first + mk(h * i, h * j, h * kk);
         float v = 0.f;
         int f = 3;
-        if (!overflow) f = warp_point_f(P, W, pc, p, live, float(clamp), lane, &v, &lastk, &ls, &lt, qz);
+        if (!overflow)
+          f = warp_point_f(P, W, pc, p, live, float(clamp), lane, &v, &lastk, &ls, &lt, qz, &n_evals, &n_solves);
         if (!live) continue;
         S.flag[nn] = int8_t(f);
         if (f == 3) {
@@ -265,7 +331,7 @@ __global__ void __launch_bounds__(MW * 32, ICAM_MIXED_BLOCKS) k_bricks_m(BrickAr
       }
       __syncwarp();
       // the double walk's list: the same candidates, centre starts (no seeds)
-      const WarpCands W64{S.code, S.lb64, S.cert, nullptr, nullptr, S.net, S.net32, n, overflow};
+      const WarpCands W64{S.code, S.lb64, net_w ? S.lbs : nullptr, S.cert, nullptr, nullptr, S.net, S.net32, n, overflow};
       int tail = 0;
       for (int b0 = 0; b0 < npend; b0 += 32) {
         const bool live = b0 + lane < npend;
@@ -310,9 +376,17 @@ __global__ void __launch_bounds__(MW * 32, ICAM_MIXED_BLOCKS) k_bricks_m(BrickAr
     int provisional = 0;
     if (a.words_out || a.kind_out)
       provisional = brick_post<float>(S.x.w.u.f, S.flag, S.v.mk, first, h, clamp, dc, dce, n_far,
-                                      a.words_out ? a.words_out + bi * 365 : nullptr,
+                                      a.words_out ? a.words_out + bi * WORD_STRIDE : nullptr,
                                       a.kind_out ? a.kind_out + bi : nullptr, lane);
-    if (a.stats) brick_census(P, S.code, n, overflow, n_exact, n_far, n_und, provisional, a.stats, lane);
+    if (a.stats) {
+      brick_census(P, S.code, n, overflow, n_exact, n_far, n_und, provisional, a.stats, lane);
+      n_evals = __reduce_add_sync(FULL, n_evals);
+      n_solves = __reduce_add_sync(FULL, n_solves);
+      if (lane == 0 && n_solves) {
+        atomicAdd(&a.stats[16], (unsigned long long)n_evals);
+        atomicAdd(&a.stats[17], (unsigned long long)n_solves);
+      }
+    }
     __syncwarp();
   }
 }

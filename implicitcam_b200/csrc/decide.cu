@@ -206,7 +206,7 @@ __device__ __forceinline__ void decide_group(const DecideArgs& a, const Box4* bo
       S.slot[k] = int8_t(slot);
     }
     __syncwarp();
-    const WarpCands W{S.code, S.lb, S.cert, S.slot, S.seed, S.net, S.net32, nc, overflow};
+    const WarpCands W{S.code, S.lb, nullptr, S.cert, S.slot, S.seed, S.net, S.net32, nc, overflow};
     double vv;
     int ff;
     warp_point<false>(P, W, c, gc, live && mine, cut, lane, &vv, &ff);
@@ -385,7 +385,7 @@ __device__ __forceinline__ void decide_group_f(const DecideArgs& a, const Box4* 
         for (int k = lane; k < nc; k += 32) rs[k] = -1;
         __syncwarp();
       }
-      const WarpCandsF W{S.code, S.lbf, S.cert, S.slot, S.seed, S.u.geo, S.net32, S.res, rs, nc, 16};
+      const WarpCandsF W{S.code, S.lbf, S.lbf, S.cert, S.slot, S.seed, S.u.geo, S.net32, S.res, rs, nc, 16};
       int lastk = -1;
       float ls = 0.f, lt = 0.f;
       ff = warp_point_f(P, W, f3(float(c.x - gc.x), float(c.y - gc.y), float(c.z - gc.z)), c, mlive, float(cut),
@@ -400,7 +400,7 @@ __device__ __forceinline__ void decide_group_f(const DecideArgs& a, const Box4* 
     }
     const bool pd = mlive && f == 3;
     if (__any_sync(FULL, pd)) {  // the double walk over the same candidates, centre starts
-      const WarpCands W64{S.code, S.lb, S.cert, nullptr, nullptr, S.net, S.net32, nc, overflow};
+      const WarpCands W64{S.code, S.lb, nullptr, S.cert, nullptr, nullptr, S.net, S.net32, nc, overflow};
       double v64;
       int f64;
       warp_point<false>(P, W64, c, gc, pd, cut, lane, &v64, &f64);

@@ -515,10 +515,12 @@ HD SEf eval_bicubic_f(const float4* cp, float s, float t) {
 // 1e-6 of the square; the double polish takes it from there.
 // *last: the patch at the point of the last step's start (within that step of the end).
 // Returns whether it converged (a step under 1e-6, or both parameters held).
-HDI bool newton_bicubic_f(const float4* cp, float3 p, float* ps_, float* pt_, int iters, SEf* last) {
+HDI bool newton_bicubic_f(const float4* cp, float3 p, float* ps_, float* pt_, int iters, SEf* last,
+                          int* evals = nullptr) {
   float s = *ps_, t = *pt_;
   bool conv = false;
   for (int it = 0; it < iters; it++) {
+    if (evals) ++*evals;
     SEf e = eval_bicubic_f(cp, s, t);
     *last = e;
     float3 r = f3(e.p.x - p.x, e.p.y - p.y, e.p.z - p.z);

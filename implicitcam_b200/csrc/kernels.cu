@@ -42,7 +42,7 @@ __global__ void k_assemble(const int64_t* idx, const int32_t* kind, const int64_
     int k = kind[i];
     if (threadIdx.x == 0) map[idx[i]] = k == 1 ? 0xffffffffu : (k == 2 ? 0xfffffffeu : uint32_t(slot[i]));
     if (k == 0 && atlas)
-      for (int w = threadIdx.x; w < 365; w += blockDim.x) atlas[slot[i] * 365 + w] = words[i * 365 + w];
+      for (int w = threadIdx.x; w < 365; w += blockDim.x) atlas[slot[i] * 365 + w] = words[i * WORD_STRIDE + w];
   }
 }
 

@@ -9,6 +9,12 @@
 
 namespace icam {
 
+constexpr int kStatCount = 24;  // counters of the brick kernel (BrickArgs::stats)
+// A brick's packed words in the brick kernels' output (BrickArgs::words_out): the 365 of
+// the layout padded to 368, so that every brick starts on a 16-byte boundary and a lane
+// stores four words (eight nodes) at once, 128-bit and coalesced.
+constexpr int WORD_STRIDE = 368;
+
 // A box of bricks being decided: its first brick, its parent's signed distance at the
 // parent's centre (NaN when not known) and how far that centre is from its own.
 struct Box4 {
@@ -47,12 +53,13 @@ struct BrickArgs {
   const void* net_w;      //   (seednet.cuh), or null: centre starts
   double* d_out;          // optional n x 729 values
   int8_t* flag_out;       // optional n x 729 flags
-  uint32_t* words_out;    // optional n x 365 packed words
+  uint32_t* words_out;    // optional n x WORD_STRIDE packed words (365 used)
   int32_t* kind_out;      // optional n kinds (0 words, 1 air, 2 solid)
   // exact, far, undecided, bridged, pairs, overflows, census [6..10], bricks given their
-  // kind from the centre alone [11], nodes the mixed kernel read in double precision [12];
-  // [15] the kernel's brick counter. Zeroed before each launch; null for none (bricks
-  // then taken in a fixed order).
+  // kind from the centre alone [11], nodes the mixed kernel read in double precision [12],
+  // a bulk copy that timed out [13]; [15] the kernel's brick counter; the mixed kernel's
+  // float Newton iterations [16] and solves [17]. kStatCount counters, zeroed before each
+  // launch; null for none (bricks then taken in a fixed order).
   unsigned long long* stats;
 };
 

@@ -141,6 +141,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int li
 struct WarpCandsF {
   const uint32_t* code;
   const float* lb;
+  const float* lbs;    // the least bound from each candidate on (the walk's exit): lb when ranked by it
   const int8_t* cert;
   const int8_t* slot;
   const SeedF* seed;
@@ -162,7 +163,7 @@ struct WarpCandsF {
 // where such a distance and its opposite both round to zero); 0 otherwise.
 __device__ __forceinline__ int warp_point_f(const DPack& P, const WarpCandsF& W, float3 pc, double3 p, bool live,
                                             float cap, int lane, float* value, int* lastk, float* ls, float* lt,
-                                            float qzero = 0.f) {
+                                            float qzero = 0.f, int* n_evals = nullptr, int* n_solves = nullptr) {
   const float rr = sqrtf(dotf(pc, pc));
   // the cap widened by the float error: a node the walk finds nothing for is past the
   // cap in exact arithmetic too (flag 1); one found just past it keeps its value (flag 0)
@@ -179,7 +180,7 @@ __device__ __forceinline__ int warp_point_f(const DPack& P, const WarpCandsF& W,
   int nd = 0;
   for (int k = 0; k < W.n; k++) {
     const float lbc = W.lb[k];
-    if (__all_sync(FULL, lbc - rr >= best)) break;  // ranked: nothing later is nearer
+    if (__all_sync(FULL, W.lbs[k] - rr >= best)) break;  // nothing from here on is nearer
     const uint32_t code = W.code[k];
     const uint32_t kind = code >> IK_SHIFT, idx = code & IK_MASK;
     const float4* net = W.net32;
@@ -230,7 +231,8 @@ __device__ __forceinline__ int warp_point_f(const DPack& P, const WarpCandsF& W,
         seed_params_f(W.seed[W.slot[k]], pc, &sf, &tf);
       }
       SEf ef;
-      if (!newton_bicubic_f(net, q, &sf, &tf, W.iters, &ef)) {  // stalled: the double walk
+      if (n_solves) ++*n_solves;
+      if (!newton_bicubic_f(net, q, &sf, &tf, W.iters, &ef, n_evals)) {  // stalled: the double walk
         pend = true;
         best = -1.f;
         continue;

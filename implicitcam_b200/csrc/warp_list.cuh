@@ -222,6 +222,7 @@ static __device__ __noinline__ bool sub_convex_at(const DSub& s, double3 p) { re
 struct WarpCands {
   const uint32_t* code;
   const double* lb;
+  const float* lbs;  // the least bound from each candidate on, rounded down (null: lb, ranked by it)
   const int8_t* cert;
   const int8_t* slot;
   const Seed* seed;
@@ -258,7 +259,8 @@ __device__ __forceinline__ void warp_point(const DPack& P, const WarpCands& W, d
   };
   for (int k = 0; k < W.n && !W.overflow; k++) {
     const double lbc = W.lb[k];
-    if (__all_sync(FULL, lbc - rr >= best)) break;  // ranked: nothing later is nearer
+    const double lbk = W.lbs ? double(W.lbs[k]) : lbc;
+    if (__all_sync(FULL, lbk - rr >= best)) break;  // nothing from here on is nearer
     const uint32_t code = W.code[k];
     const uint32_t kind = code >> IK_SHIFT, idx = code & IK_MASK;
     if (kind == IK_SUB) {  // the control net to shared memory, by the whole warp

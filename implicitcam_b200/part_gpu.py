@@ -35,7 +35,8 @@ class IcamBakeStats(C.Structure):
         ("pairs", C.c_int64), ("fallback_nodes", C.c_int64), ("kernel_launches", C.c_int64),
         ("ms_decide", C.c_double), ("ms_cull", C.c_double), ("ms_nodes", C.c_double), ("ms_post", C.c_double),
         ("census", C.c_int64 * 5), ("bricks_settled", C.c_int64), ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64),
-        ("nodes_double", C.c_int64), ("centres_double", C.c_int64),
+        ("nodes_double", C.c_int64), ("centres_double", C.c_int64), ("newton_solves", C.c_int64),
+        ("newton_evals", C.c_int64),
     ]
 
     def as_dict(self):

@@ -90,6 +90,9 @@ typedef struct IcamBakeStats {
   /* The mixed forms: box centres the decision's float reading left to the double walk
    * (a verdict within the float error of its threshold, a value near zero). */
   int64_t centres_double;
+  /* The mixed forms' brick kernel: single-precision Newton solves of sub-patches at the
+   * nodes, and the patch evaluations they took (the iterations). */
+  int64_t newton_solves, newton_evals;
 } IcamBakeStats;
 
 /* Packs the solid for the device (PartGpu::new, partgpu.rs:132; Exact::gpu_pack,
