@@ -241,6 +241,9 @@ def main():
                     help="freeform: the headline (h 0.1 mm, band 2 mm); mold: the mold cavity's pocket "
                          "(h 0.05 mm, band 1 mm); batch: 64 seeded uneven parts at h = 0.2 mm baked together; "
                          "block: the block with a hole's point queries and levels")
+    ap.add_argument("--shard", action="store_true",
+                    help="under torchrun: the ranks bake ONE level together (each rank a box of it, maps and "
+                         "atlases all-gathered over NCCL; strong scaling) instead of a part each")
     ap.add_argument("--seednet-steps", type=int, default=SEEDNET_STEPS,
                     help="training steps of the seed network (fewer only for profiling captures)")
     args = ap.parse_args()
@@ -255,6 +258,8 @@ def main():
         return run_batch(args, rank, world)
     if args.workload == "block":
         return run_block(args, rank, world)
+    if args.shard:
+        return run_shard(args, rank, world, local)
 
     import torch
 
@@ -404,6 +409,86 @@ def main():
         print(json.dumps(out), flush=True)
     g.close()
     if dist:
+        dist.destroy_process_group()
+
+
+def run_shard(args, rank, world, local):
+    """One level (the freeform part of seed 0 or the mold's pocket) baked by all ranks
+    together (implicitcam_b200/shard.py): the level cut once into a box a rank by k-d
+    bisection of its first-box tiles weighted by the surface within their reach; each
+    step every rank bakes its box, reads it into device tensors, all-gathers the maps and
+    atlases over NCCL and assembles the whole level. Strong scaling: the level is fixed.
+    The step's time is the slowest rank's, CUDA events around the step on torch's stream
+    (the bake itself returns when its stream is done)."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    from implicitcam_b200 import part_gpu, shard
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    prec = {"fp64": part_gpu.FP64, "mixed": part_gpu.MIXED, "learned": part_gpu.MIXED_LEARNED}[args.precision]
+    b, lo, nb = workload(seed=0, kind=args.workload)
+    need = BAND + 8 * H * np.sqrt(3.0)
+    g = part_gpu.PartGpu(b, need=need, device=local)
+    if prec == part_gpu.MIXED_LEARNED:  # every rank trains the same net (same seed)
+        g.seednet_train(args.seednet_steps, batch=SEEDNET_BATCH, seed=0, need=need)
+    size, start, dims = shard.tile_grid(H, lo, nb)
+    w = shard.tile_weights(lambda p: g.points(p)[0], H, lo, nb, BAND)
+    boxes = shard.plan(w, size, start, nb, world)
+    org = shard.level_origin(H, lo)
+    lo_r, nb_r = shard.sub_level(H, lo, boxes[rank])
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def step():
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        if (nb_r > 0).all():
+            mr, ar = g.level_torch(H, lo_r, nb_r, BAND, origin=org, precision=prec)
+        else:
+            mr = torch.zeros(0, dtype=torch.int32, device=dev)
+            ar = torch.zeros((0, part_gpu.WORDS), dtype=torch.int32, device=dev)
+        if world > 1:
+            maps, atlases = shard.exchange(dist, boxes, mr, ar)
+        else:
+            maps, atlases = [mr], [ar]
+        M, A = shard.assemble(nb, boxes, maps, atlases)
+        e1.record()
+        e1.synchronize()
+        return e0.elapsed_time(e1), M, A
+
+    for _ in range(args.warmup):
+        step()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ms = 0.0
+    for _ in range(args.steps):
+        t, M, A = step()
+        ms += t
+    torch.cuda.synchronize()
+    bricks_read = int(g.decide(H, lo, nb, BAND, precision=prec)[3]["bricks_read"])
+    total_ms, _ = over_ranks(dist if world > 1 else None, dev, ms)
+    if rank == 0:
+        out = {"metric": METRIC, "value": 512.0 * bricks_read * args.steps / (total_ms * 1e-3), "unit": "voxels/s",
+               "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+               "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+               "dtype": "f64" if prec == part_gpu.FP64 else "f32+f64", "data": "synthetic",
+               "config": {"workload": workload_name(args.workload) + ", one level over all ranks",
+                          "h_mm": H, "band_mm": BAND, "nb": nb.tolist(), "precision": args.precision,
+                          "parallelism": f"level cut into {world} boxes, maps and atlases all-gathered",
+                          "l2": "flushed (256 MB write) before every step"},
+               "boxes": [[b0.tolist(), b1.tolist()] for b0, b1 in boxes],
+               "stored_bricks": int(A.shape[0]), "gpu_launches": None}
+        print(json.dumps(out), flush=True)
+    g.close()
+    if world > 1:
         dist.destroy_process_group()
 
 

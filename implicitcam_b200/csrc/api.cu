@@ -618,10 +618,12 @@ int icam_level_read(IcamPack* pk, uint32_t* map_out, size_t map_entries, uint32_
   if (atlas_out && atlas_cap_words < pk->last_slots * 365)
     return fail(pk, ICAM_ERR_ARG, "icam_level_read: atlas_out holds fewer than n_slots x 365 words");
   CK(cudaSetDevice(pk->device));
+  // the direction inferred from the addresses (unified addressing): host arrays, or
+  // device memory of this GPU or a peer (a caller that keeps the level on the device)
   if (map_out)
-    CK(cudaMemcpyAsync(map_out, pk->last_map, map_entries * sizeof(uint32_t), cudaMemcpyDeviceToHost, pk->stream));
+    CK(cudaMemcpyAsync(map_out, pk->last_map, map_entries * sizeof(uint32_t), cudaMemcpyDefault, pk->stream));
   if (atlas_out && pk->last_slots)
-    CK(cudaMemcpyAsync(atlas_out, pk->last_atlas, pk->last_slots * 365 * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+    CK(cudaMemcpyAsync(atlas_out, pk->last_atlas, pk->last_slots * 365 * sizeof(uint32_t), cudaMemcpyDefault,
                        pk->stream));
   CK(cudaStreamSynchronize(pk->stream));
   return ICAM_OK;

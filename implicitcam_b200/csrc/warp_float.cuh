@@ -184,17 +184,18 @@ __device__ __forceinline__ int warp_point_f(const DPack& P, const WarpCandsF& W,
     const uint32_t code = W.code[k];
     const uint32_t kind = code >> IK_SHIFT, idx = code & IK_MASK;
     const float4* net = W.net32;
+    const bool want = lbc - rr < best;
     if (kind == IK_SUB) {
       const int rs = W.rslot[k];
       if (rs >= 0) {
         net = W.res + 16 * rs;
-      } else {  // not resident: to shared memory by the whole warp
+      } else if (__any_sync(FULL, want)) {  // not resident: to shared memory by the whole warp
         __syncwarp();
         if (lane < 16) W.net32[lane] = P.sub_cp32[16 * size_t(idx) + lane];
         __syncwarp();
       }
     }
-    if (lbc - rr >= best) continue;
+    if (!want) continue;
     const float4 g0 = W.geo[2 * k];
     if (kind == IK_FACE && !isnan(g0.w)) {  // a plane
       const int8_t ct = W.cert[k];

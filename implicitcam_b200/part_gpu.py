@@ -128,6 +128,7 @@ class PartGpu:
         assert isinstance(desc, IcamSolidDesc)
         self._solid = solid
         self._desc = desc
+        self.device = device
         opt = IcamPackOptions(device, need)
         h = C.c_void_p()
         err = C.create_string_buffer(1024)
@@ -247,6 +248,27 @@ class PartGpu:
                                           ptr(map_out), ptr(atlas_out), words(atlas_out), C.byref(ns), C.byref(st)),
                     "icam_bake_level")
         return ns.value, st.as_dict()
+
+    def level_torch(self, h, lo, nb, clamp=None, origin=None, precision=FP64):
+        """The bake read into torch tensors on the pack's device (one bake, then one
+        device-to-device read): (map int32 (the u32 entries), atlas int32 slots x 365)."""
+        import torch
+
+        lo = np.ascontiguousarray(lo, dtype=np.float64)
+        nb = np.ascontiguousarray(nb, dtype=np.int64)
+        clamp = h * np.sqrt(3.0) if clamp is None else clamp
+        org = None if origin is None else np.ascontiguousarray(origin, dtype=np.float64)
+        ns = C.c_size_t()
+        st = IcamBakeStats()
+        self._check(lib().icam_bake_level(self.h, float(h), _p(lo), _p(nb), float(clamp), _p(org), precision, None,
+                                          None, 0, C.byref(ns), C.byref(st)), "icam_bake_level")
+        dev = torch.device("cuda", self.device)
+        m = torch.empty(int(np.prod(nb)), dtype=torch.int32, device=dev)
+        a = torch.empty((ns.value, WORDS), dtype=torch.int32, device=dev)
+        self._check(lib().icam_level_read(self.h, C.c_void_p(m.data_ptr()), m.numel(),
+                                          C.c_void_p(a.data_ptr()) if ns.value else None, a.numel()),
+                    "icam_level_read")
+        return m, a
 
     def level_device(self, h, lo, nb, clamp=None, origin=None, precision=FP64):
         """The same bake with its results left on the device: (map ptr, atlas ptr, slots, stats)."""

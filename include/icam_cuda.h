@@ -170,10 +170,12 @@ int icam_decide_level(IcamPack* pack, double h, const double lo[3], const int64_
                       size_t read_cap, size_t* n_read, IcamBakeStats* stats);
 
 /* The last level baked on the pack (by icam_bake_level or icam_bake_level_device),
- * copied to host arrays without baking again: map_out (map_entries = the level's
+ * copied out without baking again: map_out (map_entries = the level's
  * nb[0]*nb[1]*nb[2] entries) and atlas_out (atlas_cap_words >= n_slots x 365), either
  * may be NULL. The sizing pattern is one bake with atlas_out NULL for *n_slots, then
- * this read into an atlas of that size. No counterpart in the reference, whose level
+ * this read into an atlas of that size. The outputs may be host arrays or device memory
+ * (the copy's direction follows from the addresses), so a caller that keeps the level on
+ * its GPUs reads it into buffers of its own. No counterpart in the reference, whose level
  * bake returns owned vectors. ICAM_ERR_ARG when no level was baked or a size is wrong. */
 int icam_level_read(IcamPack* pack, uint32_t* map_out, size_t map_entries, uint32_t* atlas_out,
                     size_t atlas_cap_words);
