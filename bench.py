@@ -57,15 +57,15 @@ def set_level(h, band):
 
 
 def workload(seed: int, kind: str = "freeform"):
-    """The part and its level's (lo, nb): the freeform top's whole box, or the mold
-    cavity's pocket (its floor of 500 B-spline faces and the walls' lower parts)."""
+    """The part and its level's (lo, nb), over the part's whole box: the freeform top,
+    or the mold cavity (its block, the pocket's floor of 500 B-spline faces, the bosses
+    on its rim)."""
     from implicitcam_b200 import parts
 
     if kind == "mold":
         b = parts.mold(seed=seed)
-        net = np.concatenate([np.asarray(p).reshape(-1, 4) for p in b.patches])
-        xyz = net[:, :3] / net[:, 3:]  # the floor lies within its control points
-        lo, hi = xyz.min(0), xyz.max(0)
+        pts = np.asarray(b.verts)  # the block's corners and the bosses' caps bound it
+        lo, hi = pts.min(0), pts.max(0)
     else:
         b = parts.freeform_top(seed=seed)
         # the part's box: the control net's box (the top is within its control points)
@@ -107,7 +107,8 @@ def over_ranks(dist, device, ms, voxels=None):
 
 def workload_name(kind):
     if kind == "mold":
-        return f"mold cavity pocket level bake (500 B-spline floor faces), h={H} mm, band +-{BAND} mm"
+        return (f"mold cavity level bake over the whole block (500 B-spline floor faces of 8x8-24x24 control "
+                f"points), h={H} mm, band +-{BAND} mm")
     return f"freeform-top level bake, h={H} mm, band +-{BAND} mm"
 
 
@@ -494,29 +495,38 @@ def run_shard(args, rank, world, local):
 
 def batch_parts(seed0=0, count=64):
     """Uneven seeded parts of four families, a quarter each: blocks with rational
-    B-spline tops of 4 x 4 to 32 x 32 control points and 20-120 mm sides; bosses
-    (cylinder, torus fillet, plane cap); blocks with countersunk holes (cylinder and
-    cone); spherical domes (cylinder under a hemisphere). Returns [(family, solid)]."""
+    B-spline tops of 4 x 4 to 32 x 32 control points, degree 2 or 3, weights U[0.7, 1.3],
+    cut along their knot lines into 1 to 19 faces a side (6 to 366 faces), 20-120 mm
+    sides; plates with one to four filleted bosses (cylinder, torus fillet, plane cap;
+    9 to 18 faces); blocks with countersunk holes (cylinder and cone; 8 faces); plates with
+    one to four spherical domes (cylinder under a hemisphere; 8 to 14 faces).
+    Returns [(family, solid)]."""
     from implicitcam_b200 import parts
 
     out = []
     for k in range(count):
         f = k % 4
-        if f == 0:
-            out.append(("freeform_top", parts.freeform_top(
-                seed=seed0 + k, n=4 + (7 * k) % 29, size=20.0 + (37 * k) % 100, base=10.0 + (13 * k) % 40,
-                bumps=2 + k % 7)))
+        s = seed0 + k
+        if f == 0:  # the j-th of the family: control points and faces grow with j
+            j = k // 4
+            n = 4 + (28 * j) // 15
+            deg = 2 + j % 2
+            out.append(("freeform_top", parts.freeform_patches(
+                seed=s, n=n, size=20.0 + (37 * k) % 100, base=10.0 + (13 * k) % 40, bumps=2 + k % 7, degree=deg,
+                faces=1 + (18 * j) // 15)))
         elif f == 1:
-            r = 4.0 + (5 * k) % 17
-            out.append(("boss", parts.boss(r=r, height=r + 4.0 + (3 * k) % 19, fillet=0.5 + 0.1 * ((7 * k) % 20))))
+            m = 1 + (k // 4) % 4
+            out.append(("boss", parts.bodies_on_plate(seed=s, kind="boss", count=m,
+                                                      plate=(12.0 * m + (3 * k) % 10, 14.0 + (5 * k) % 9, 4.0 + k % 5))))
         elif f == 2:
             X, Y, Z = 20.0 + (11 * k) % 80, 15.0 + (7 * k) % 50, 10.0 + (5 * k) % 30
             r = 0.12 * min(X, Y)
             out.append(("countersunk_block", parts.countersunk_block(
                 size=(X, Y, Z), center=(X / 2, Y / 2), r=r, sink=min(0.4 * r, 0.3 * Z))))
         else:
-            r = 3.0 + (7 * k) % 23
-            out.append(("dome", parts.dome(r=r, height=2.0 + (5 * k) % 21)))
+            m = 1 + (k // 4) % 4
+            out.append(("dome", parts.bodies_on_plate(seed=s, kind="dome", count=m,
+                                                      plate=(12.0 * m + (3 * k) % 10, 14.0 + (5 * k) % 9, 4.0 + k % 5))))
     return out
 
 

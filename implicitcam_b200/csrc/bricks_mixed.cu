@@ -54,6 +54,8 @@ struct BrickSmemF {
   int n;
 };
 static_assert(sizeof(((BrickSmemF*)0)->x) >= SN_ROOM, "the seed network's room");
+static_assert(sizeof(BrickSmemF) % 16 == 0 && SN_WBYTES % 16 == 0, "the staged weights are 16-byte aligned");
+static_assert(2 * (sizeof(BrickSmemF) * MW + SN_WBYTES) <= 227 * 1024, "two blocks a SM with the weights staged");
 
 // The i16 step's half: a distance below it (less the float error) rounds to zero on
 // either side of the surface, so a bake that keeps only i16 values needs no sign for it.
@@ -82,6 +84,16 @@ __global__ void __launch_bounds__(MW * 32, ICAM_MIXED_BLOCKS) k_bricks_m(BrickAr
   const int warps = int(blockDim.x >> 5);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   BrickSmemF& S = smem[warp];
+  // the seed network's weights, staged once a block behind the warps' rooms (one part
+  // a launch: a batch's parts each have their own, read from global memory)
+  const void* net_staged = nullptr;
+  if (!BATCH && a.net_w) {
+    uint4* dst = reinterpret_cast<uint4*>(smem_raw + sizeof(BrickSmemF) * warps);
+    const uint4* src = static_cast<const uint4*>(a.net_w);
+    for (int i = threadIdx.x; i < int(SN_WBYTES / 16); i += blockDim.x) dst[i] = src[i];
+    __syncthreads();
+    net_staged = dst;
+  }
   unsigned long long* work = a.stats ? a.stats + 15 : nullptr;
   if (lane == 0) mbar_init(&S.bar);
   __syncwarp();
@@ -101,7 +113,7 @@ __global__ void __launch_bounds__(MW * 32, ICAM_MIXED_BLOCKS) k_bricks_m(BrickAr
     const int32_t* leaves = BATCH ? Q->leaves : a.leaves;
     const int32_t n_leaves = BATCH ? Q->n_leaves : a.n_leaves;
     const float* net_feat = BATCH ? Q->net_feat : a.net_feat;
-    const void* net_w = BATCH ? Q->net_w : a.net_w;
+    const void* net_w = BATCH ? Q->net_w : net_staged;
     const double3 first = mk(a.firsts[3 * bi], a.firsts[3 * bi + 1], a.firsts[3 * bi + 2]);
     const double half = 4.0 * h;
     const double3 c = first + mk(half, half, half);
@@ -397,10 +409,10 @@ void launch_bricks_mixed(const BrickArgs& a, cudaStream_t s, int warps) {
   warps = warps == 1 || warps == 2 ? warps : MW;
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const size_t smem = sizeof(BrickSmemF) * warps;
   const bool batch = a.parts != nullptr;
+  const size_t smem = sizeof(BrickSmemF) * warps + (!batch && a.net_w ? SN_WBYTES : 0);
   auto kern = batch ? k_bricks_m<true> : k_bricks_m<false>;
-  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(BrickSmemF) * MW));
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(BrickSmemF) * MW + SN_WBYTES));
   int per_sm = 1;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, warps * 32, smem);
   const int64_t want = (a.n + warps - 1) / warps;

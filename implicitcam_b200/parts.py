@@ -251,6 +251,109 @@ def _nurbs_box(b: SolidBuilder, du, dv, ku, kv, net_h, X, Y, top_sense=+1):
     return b
 
 
+def _spline_faces(b: SolidBuilder, patches, ub, vb, cu, cv, sense=+1):
+    """One B-spline surface (its Bezier spans `patches` (NU, NV, ..), breaks ub, vb) cut
+    along span boundaries into faces: face (a, c) holds spans cu[a]..cu[a+1]-1 by
+    cv[c]..cv[c+1]-1 (cu, cv increasing from 0 to NU, NV). Neighbouring faces share their
+    vertices and iso-curve edges, so they join as the surface does. Returns the vertices
+    fvx[a, c] at the cut grid and the edges eu[a, c] (u = ub[cu[a]], along v over face
+    row c) and ev[a, c] (v = vb[cv[c]], along u over face column a), each stored in
+    increasing parameter."""
+    NU, NV = patches.shape[:2]
+    FU, FV = len(cu) - 1, len(cv) - 1
+    pt = lambda hh: hh[:3] / hh[3]  # noqa: E731
+    fvx = {}
+    for a in range(FU + 1):
+        for c in range(FV + 1):
+            i, j = min(cu[a], NU - 1), min(cv[c], NV - 1)
+            fvx[a, c] = b.vertex(pt(patches[i, j, -1 if cu[a] == NU else 0, -1 if cv[c] == NV else 0]))
+    eu, ev = {}, {}
+    for a in range(FU + 1):
+        for c in range(FV):
+            i = cu[a]
+            pieces = [(patches[i, j, 0] if i < NU else patches[NU - 1, j, -1]).copy() for j in range(cv[c], cv[c + 1])]
+            eu[a, c] = b.spline(pieces, fvx[a, c], fvx[a, c + 1])
+    for a in range(FU):
+        for c in range(FV + 1):
+            j = cv[c]
+            pieces = [(patches[i, j, :, 0] if j < NV else patches[i, NV - 1, :, -1]).copy() for i in range(cu[a], cu[a + 1])]
+            ev[a, c] = b.spline(pieces, fvx[a, c], fvx[a + 1, c])
+    for a in range(FU):
+        for c in range(FV):
+            i0, i1, j0, j1 = cu[a], cu[a + 1], cv[c], cv[c + 1]
+            u0, u1, v0, v1 = ub[i0], ub[i1], vb[j0], vb[j1]
+            f = b.face(NURBS, sense, lo=[u0, v0], hi=[u1, v1],
+                       nurbs=(patches[i0:i1, j0:j1].copy(), np.asarray(ub[i0:i1 + 1]).copy(),
+                              np.asarray(vb[j0:j1 + 1]).copy()))
+            b.loop(f, [
+                (ev[a, c], False, line_pcurve([u0, v0], [u1, v0])),
+                (eu[a + 1, c], False, line_pcurve([u1, v0], [u1, v1])),
+                (ev[a, c + 1], True, line_pcurve([u1, v1], [u0, v1])),
+                (eu[a, c], True, line_pcurve([u0, v1], [u0, v0])),
+            ])
+    return fvx, eu, ev
+
+
+def _patched_box(b: SolidBuilder, du, dv, ku, kv, net_h, X, Y, cu, cv):
+    """_nurbs_box with its top cut into faces along span boundaries (_spline_faces):
+    a block [0,X]x[0,Y]x[0,top], the top a clamped rational B-spline of degrees (du, dv)
+    cut into (len(cu) - 1) x (len(cv) - 1) faces, four side planes and a bottom plane."""
+    patches, ub, vb = surface_spans(du, dv, ku, kv, net_h)
+    fvx, eu, ev = _spline_faces(b, patches, ub, vb, cu, cv)
+    FU, FV = len(cu) - 1, len(cv) - 1
+    c = {}
+    for i, x in enumerate((0.0, X)):
+        for j, y in enumerate((0.0, Y)):
+            c[i, j, 0] = b.vertex([x, y, 0.0])
+    c[0, 0, 1], c[1, 0, 1], c[1, 1, 1], c[0, 1, 1] = fvx[0, 0], fvx[FU, 0], fvx[FU, FV], fvx[0, FV]
+    L = lambda p, q: b.line(c[p], c[q])  # noqa: E731
+    eb = [L((0, 0, 0), (1, 0, 0)), L((1, 0, 0), (1, 1, 0)), L((1, 1, 0), (0, 1, 0)), L((0, 1, 0), (0, 0, 0))]
+    es = {ij: L((*ij, 0), (*ij, 1)) for ij in ((0, 0), (1, 0), (1, 1), (0, 1))}
+    _plane_face(b, Frame([0, 0, 0], [0, 0, 1], [1, 0, 0]), -1,
+                [[(eb[3], True), (eb[2], True), (eb[1], True), (eb[0], True)]])
+    _plane_face(b, Frame([0, 0, 0], [0, -1, 0], [1, 0, 0]), +1,
+                [[(eb[0], False), (es[1, 0], False)] + [(ev[a, 0], True) for a in reversed(range(FU))]
+                 + [(es[0, 0], True)]])
+    _plane_face(b, Frame([X, 0, 0], [1, 0, 0], [0, 1, 0]), +1,
+                [[(eb[1], False), (es[1, 1], False)] + [(eu[FU, cc], True) for cc in reversed(range(FV))]
+                 + [(es[1, 0], True)]])
+    _plane_face(b, Frame([X, Y, 0], [0, 1, 0], [-1, 0, 0]), +1,
+                [[(eb[2], False), (es[0, 1], False)] + [(ev[a, FV], False) for a in range(FU)] + [(es[1, 1], True)]])
+    _plane_face(b, Frame([0, Y, 0], [-1, 0, 0], [0, -1, 0]), +1,
+                [[(eb[3], False), (es[0, 0], False)] + [(eu[0, cc], False) for cc in range(FV)] + [(es[0, 1], True)]])
+    return b
+
+
+def _even_cuts(spans, faces):
+    """`faces` + 1 cut indices from 0 to `spans`, as even as the spans allow."""
+    faces = max(1, min(faces, spans))
+    return [round(spans * k / faces) for k in range(faces + 1)]
+
+
+def freeform_patches(seed=0, n=16, size=120.0, base=50.0, bumps=8, degree=3, faces=4):
+    """The freeform top of freeform_top, of any degree (2 or 3; weights U[0.7, 1.3]),
+    cut along its knot lines into faces x faces B-spline faces (as even as its n - degree
+    spans a side allow) that join C^(degree-1) along shared B-spline edges: faces^2 + 5
+    faces in all."""
+    rng = Rng(seed)
+    g = []
+    for _ in range(bumps):
+        g.append((rng.uniform(2.0, 6.0), rng.uniform(8.0, 25.0), rng.uniform(0.0, size), rng.uniform(0.0, size)))
+    step = size / (n - 1)
+    net = np.zeros((n, n, 4))
+    for i in range(n):
+        for j in range(n):
+            x, y = step * i, step * j
+            z = base + sum(a * math.exp(-((x - cx) ** 2 + (y - cy) ** 2) / (2 * s * s)) for a, s, cx, cy in g)
+            w = rng.uniform(0.7, 1.3)
+            net[i, j] = [x * w, y * w, z * w, w]
+    spans = n - degree
+    knots = [0.0] * (degree + 1) + [k / spans for k in range(1, spans)] + [1.0] * (degree + 1)
+    cuts = _even_cuts(spans, faces)
+    b = SolidBuilder(tol=1e-9)
+    return _patched_box(b, degree, degree, knots, knots, net, size, size, cuts, cuts)
+
+
 def bump_box():
     """The reference test's bump box (solid3.rs:2092-2147): a 10 x 10 box whose top
     is a biquadratic B-spline over the square, z(5i, 5j) control heights zc."""
@@ -413,6 +516,76 @@ def dome(r=3.0, height=4.0):
     return b
 
 
+def _dome_body(b: SolidBuilder, cx, cy, z0, r, height):
+    """A dome standing on the plane z = z0: a cylinder of radius r to z0 + height capped by
+    the hemisphere on its top circle. Returns its base circle, a hole loop for the plane."""
+    z, x = [0, 0, 1], [1, 0, 0]
+    f0, f1 = Frame([cx, cy, z0], z, x), Frame([cx, cy, z0 + height], z, x)
+    va, vb = b.vertex([cx + r, cy, z0]), b.vertex([cx + r, cy, z0 + height])
+    c0 = b.arc(f0, r, 0.0, TAU, va, va)
+    c1 = b.arc(f1, r, 0.0, TAU, vb, vb)
+    seam = b.line(va, vb)
+    lo, hi = _pad([0.0, 0.0], [TAU, height])
+    cyl = b.face(CYLINDER, +1, f0, a=r, lo=[0.0, lo[1]], hi=[TAU, hi[1]], period=[TAU, 0.0])
+    b.loop(cyl, [
+        (c0, False, line_pcurve([0.0, 0.0], [TAU, 0.0])),
+        (seam, False, None),
+        (c1, True, line_pcurve([TAU, height], [0.0, height])),
+        (seam, True, None),
+    ])
+    lo, hi = _pad([0.0, 0.0], [TAU, math.pi / 2])
+    sph = b.face(SPHERE, +1, f1, a=r, lo=[0.0, lo[1]], hi=[TAU, hi[1]], period=[TAU, 0.0])
+    b.loop(sph, [(c1, False, line_pcurve([0.0, 0.0], [TAU, 0.0]))])
+    return c0
+
+
+def _plate(b: SolidBuilder, X, Y, Z, holes):
+    """A plate [0,X]x[0,Y]x[0,Z] whose top face has the given hole loops (the base circles
+    of bodies standing on it): bottom, four sides and the top."""
+    c = {}
+    for i, xx in enumerate((0.0, X)):
+        for j, yy in enumerate((0.0, Y)):
+            for k, zz in enumerate((0.0, Z)):
+                c[i, j, k] = b.vertex([xx, yy, zz])
+    L = lambda p, q: b.line(c[p], c[q])  # noqa: E731
+    eb = [L((0, 0, 0), (1, 0, 0)), L((1, 0, 0), (1, 1, 0)), L((1, 1, 0), (0, 1, 0)), L((0, 1, 0), (0, 0, 0))]
+    et = [L((0, 0, 1), (1, 0, 1)), L((1, 0, 1), (1, 1, 1)), L((1, 1, 1), (0, 1, 1)), L((0, 1, 1), (0, 0, 1))]
+    es = {ij: L((*ij, 0), (*ij, 1)) for ij in ((0, 0), (1, 0), (1, 1), (0, 1))}
+    _plane_face(b, Frame([0, 0, 0], [0, 0, 1], [1, 0, 0]), -1,
+                [[(eb[3], True), (eb[2], True), (eb[1], True), (eb[0], True)]])
+    _plane_face(b, Frame([0, 0, 0], [0, -1, 0], [1, 0, 0]), +1,
+                [[(eb[0], False), (es[1, 0], False), (et[0], True), (es[0, 0], True)]])
+    _plane_face(b, Frame([X, 0, 0], [1, 0, 0], [0, 1, 0]), +1,
+                [[(eb[1], False), (es[1, 1], False), (et[1], True), (es[1, 0], True)]])
+    _plane_face(b, Frame([X, Y, 0], [0, 1, 0], [-1, 0, 0]), +1,
+                [[(eb[2], False), (es[0, 1], False), (et[2], True), (es[1, 1], True)]])
+    _plane_face(b, Frame([0, Y, 0], [-1, 0, 0], [0, -1, 0]), +1,
+                [[(eb[3], False), (es[0, 0], False), (et[3], True), (es[0, 1], True)]])
+    _plane_face(b, Frame([0, 0, Z], [0, 0, 1], [1, 0, 0]), +1,
+                [[(et[0], False), (et[1], False), (et[2], False), (et[3], False)]] + [[(h, True)] for h in holes])
+    return b
+
+
+def bodies_on_plate(seed=0, kind="boss", count=2, plate=(40.0, 30.0, 8.0)):
+    """`count` bodies standing in a row on a plate: filleted bosses (kind "boss": cylinder,
+    quarter-torus fillet, cap; radius U[2,5] mm, height U[3,12] mm) or domes ("dome":
+    cylinder under a hemisphere; radius U[2,5] mm, cylinder height U[1,6] mm). The plate
+    and its bodies are one solid: 6 + 3 count faces (bosses) or 6 + 2 count (domes)."""
+    rng = Rng(seed)
+    X, Y, Z = plate
+    b = SolidBuilder(tol=1e-9)
+    holes = []
+    for k in range(count):
+        cx, cy = X * (k + 0.5) / count, Y / 2
+        r = min(rng.uniform(2.0, 5.0), 0.45 * min(X / count, Y))
+        if kind == "boss":
+            hgt = rng.uniform(3.0, 12.0)
+            holes.append(_boss_body(b, cx, cy, Z, r, hgt, min(0.3 * r, 0.4 * hgt) * rng.uniform(0.5, 1.0)))
+        else:
+            holes.append(_dome_body(b, cx, cy, Z, r, rng.uniform(1.0, 6.0)))
+    return _plate(b, X, Y, Z, holes)
+
+
 def countersunk_block(size=(40.0, 30.0, 20.0), center=(20.0, 15.0), r=4.0, sink=2.0, half_angle_deg=45.0):
     """A block [0,X]x[0,Y]x[0,Z] with a through-hole of radius r along z whose top
     `sink` mm widens as a cone (the countersink) to r + sink tan(angle) at z = Z."""
@@ -472,61 +645,40 @@ def countersunk_block(size=(40.0, 30.0, 20.0), center=(20.0, 15.0), r=4.0, sink=
     return b
 
 
-def mold(seed=0, size=(250.0, 200.0, 80.0), rim=25.0, fu=25, fv=20, floor=40.0, bumps=10, bosses=40):
+def mold(seed=0, size=(250.0, 200.0, 80.0), rim=25.0, fu=25, fv=20, floor=40.0, bumps=10, bosses=40,
+         spans=(5, 21)):
     """A mold cavity: a size block with a pocket `rim` mm in from its sides, the pocket's
-    floor a clamped bicubic rational B-spline of fu x fv spans (heights floor plus
-    `bumps` seeded Gaussians, amplitude U[2,8] mm, sigma U[10,40] mm; weights U[0.8,1.2])
-    cut at its knots into fu x fv faces of one span each, so neighbouring faces join C2
-    along shared B-spline edges; four vertical pocket walls; and `bosses` filleted bosses
-    (cylinder, quarter-torus fillet, cap; radius U[3,6] mm, height U[5,15] mm) standing
-    on the rim. About 640 faces."""
+    floor one clamped bicubic rational B-spline (heights floor plus `bumps` seeded
+    Gaussians, amplitude U[2,8] mm, sigma U[10,40] mm; weights U[0.8,1.2]; uniform knots)
+    cut along its knot lines into fu x fv faces: face column a holds m_u[a] spans, face row
+    c m_v[c], each drawn from `spans`, so a face is a patch of (m_u + 3) x (m_v + 3)
+    control points (8 x 8 to 24 x 24) and neighbouring faces join C2 along shared B-spline
+    edges; four vertical pocket walls; and `bosses` filleted bosses (cylinder,
+    quarter-torus fillet, cap; radius U[3,6] mm, height U[5,15] mm) standing on the rim.
+    About 640 faces."""
     X, Y, Z = size
     ax, ay, bx, by = rim, rim, X - rim, Y - rim
     rng = Rng(seed)
     g = []
     for _ in range(bumps):
         g.append((rng.uniform(2.0, 8.0), rng.uniform(10.0, 40.0), rng.uniform(ax, bx), rng.uniform(ay, by)))
-    nu, nv = fu + 3, fv + 3
-    net = np.zeros((nu, nv, 4))
-    for i in range(nu):
-        for j in range(nv):
-            x = ax + (bx - ax) * i / (nu - 1)
-            y = ay + (by - ay) * j / (nv - 1)
-            zz = floor + sum(a * math.exp(-((x - cx) ** 2 + (y - cy) ** 2) / (2 * s * s)) for a, s, cx, cy in g)
-            w = rng.uniform(0.8, 1.2)
-            net[i, j] = [x * w, y * w, zz * w, w]
-    ku = [0.0] * 4 + [k / fu for k in range(1, fu)] + [1.0] * 4
-    kv = [0.0] * 4 + [k / fv for k in range(1, fv)] + [1.0] * 4
+    mu = [spans[0] + int(rng.next() % (spans[1] - spans[0] + 1)) for _ in range(fu)]
+    mv = [spans[0] + int(rng.next() % (spans[1] - spans[0] + 1)) for _ in range(fv)]
+    su, sv = sum(mu), sum(mv)
+    nu, nv = su + 3, sv + 3
+    xs = ax + (bx - ax) * np.arange(nu) / (nu - 1)
+    ys = ay + (by - ay) * np.arange(nv) / (nv - 1)
+    XX, YY = np.meshgrid(xs, ys, indexing="ij")
+    zz = floor + sum(a * np.exp(-((XX - cx) ** 2 + (YY - cy) ** 2) / (2 * s * s)) for a, s, cx, cy in g)
+    w = np.array([rng.uniform(0.8, 1.2) for _ in range(nu * nv)]).reshape(nu, nv)
+    net = np.stack([XX * w, YY * w, zz * w, w], -1)
+    ku = [0.0] * 4 + [k / su for k in range(1, su)] + [1.0] * 4
+    kv = [0.0] * 4 + [k / sv for k in range(1, sv)] + [1.0] * 4
     patches, ub, vb = surface_spans(3, 3, ku, kv, net)
     b = SolidBuilder(tol=1e-9)
-    pt = lambda hh: hh[:3] / hh[3]  # noqa: E731
-    # the floor's vertices at its knot grid, and its iso-curve edges (increasing parameter)
-    fvx = {}
-    for a in range(fu + 1):
-        for c in range(fv + 1):
-            pa, pc = min(a, fu - 1), min(c, fv - 1)
-            fvx[a, c] = b.vertex(pt(patches[pa, pc, -1 if a == fu else 0, -1 if c == fv else 0]))
-    eu = {}  # u = ub[a], from vb[c] to vb[c + 1]
-    for a in range(fu + 1):
-        for c in range(fv):
-            piece = patches[a, c, 0, :, :] if a < fu else patches[fu - 1, c, -1, :, :]
-            eu[a, c] = b.spline([piece.copy()], fvx[a, c], fvx[a, c + 1])
-    ev = {}  # v = vb[c], from ub[a] to ub[a + 1]
-    for a in range(fu):
-        for c in range(fv + 1):
-            piece = patches[a, c, :, 0, :] if c < fv else patches[a, fv - 1, :, -1, :]
-            ev[a, c] = b.spline([piece.copy()], fvx[a, c], fvx[a + 1, c])
-    for a in range(fu):
-        for c in range(fv):
-            u0, u1, v0, v1 = ub[a], ub[a + 1], vb[c], vb[c + 1]
-            f = b.face(NURBS, +1, lo=[u0, v0], hi=[u1, v1],
-                       nurbs=(patches[a:a + 1, c:c + 1].copy(), ub[a:a + 2].copy(), vb[c:c + 2].copy()))
-            b.loop(f, [
-                (ev[a, c], False, line_pcurve([u0, v0], [u1, v0])),
-                (eu[a + 1, c], False, line_pcurve([u1, v0], [u1, v1])),
-                (ev[a, c + 1], True, line_pcurve([u1, v1], [u0, v1])),
-                (eu[a, c], True, line_pcurve([u0, v1], [u0, v0])),
-            ])
+    cu = [int(x) for x in np.concatenate([[0], np.cumsum(mu)])]
+    cv = [int(x) for x in np.concatenate([[0], np.cumsum(mv)])]
+    fvx, eu, ev = _spline_faces(b, patches, ub, vb, cu, cv)
     # the block's corners, the rim's corners at the top and the pocket walls' vertical edges
     cb = {}
     for i, xx in enumerate((0.0, X)):

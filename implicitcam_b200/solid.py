@@ -143,30 +143,41 @@ def bezier_pieces(p, knots, pts):
     return out
 
 
+def _extract_axis0(p, knots, pts):
+    """The Bezier pieces of a clamped degree-p B-spline along axis 0 of pts (every
+    other axis carried along: many curves at once), by Boehm's insertion of each
+    interior knot up to multiplicity p. Returns (pieces (spans, p+1, ...), breaks)."""
+    knots = [float(x) for x in knots]
+    pts = np.asarray(pts, dtype=np.float64)
+    for x in sorted(set(knots[p + 1:len(knots) - p - 1])):
+        while knots.count(x) < p:
+            k = max(i for i in range(len(knots) - 1) if knots[i] <= x < knots[i + 1])
+            n = len(pts)
+            i = np.arange(k - p + 1, k + 1)
+            a = (x - np.asarray(knots)[i]) / (np.asarray(knots)[i + p] - np.asarray(knots)[i])
+            a = a.reshape((-1,) + (1,) * (pts.ndim - 1))
+            mid = (1 - a) * pts[i - 1] + a * pts[i]
+            pts = np.concatenate([pts[: k - p + 1], mid, pts[k:n]], axis=0)
+            knots.insert(k + 1, x)
+    breaks = sorted(set(knots))
+    pieces = []
+    for a0 in breaks[:-1]:
+        last_a = max(i for i, x in enumerate(knots) if x == a0)
+        first = last_a - p
+        pieces.append(pts[first:first + p + 1])
+    return np.stack(pieces), np.array(breaks)
+
+
 def surface_spans(du, dv, ku, kv, net_h):
     """Bezier spans of a clamped rational B-spline surface, net_h[i][j] homogeneous
     (i along u). Returns (patches (nsu, nsv, du+1, dv+1, 4), u breaks, v breaks)."""
     net_h = np.asarray(net_h, dtype=np.float64)
-    nu, nv = net_h.shape[:2]
-    # along u for every column j
-    cols = []
-    for j in range(nv):
-        cols.append(bezier_pieces(du, ku, [net_h[i, j] for i in range(nu)]))
-    nsu = len(cols[0])
-    ub = [cols[0][0][1]] + [c[2] for c in cols[0]]
-    # then along v for every Bezier row (span a, point k)
-    rows = {}
-    for a in range(nsu):
-        for k in range(du + 1):
-            rows[(a, k)] = bezier_pieces(dv, kv, [cols[j][a][0][k] for j in range(nv)])
-    nsv = len(rows[(0, 0)])
-    vb = [rows[(0, 0)][0][1]] + [r[2] for r in rows[(0, 0)]]
-    patches = np.zeros((nsu, nsv, du + 1, dv + 1, 4))
-    for a in range(nsu):
-        for k in range(du + 1):
-            for b in range(nsv):
-                patches[a, b, k, :, :] = rows[(a, k)][b][0]
-    return patches, np.array(ub), np.array(vb)
+    # along u for every column j at once: (nsu, du+1, nv, 4)
+    pu, ub = _extract_axis0(du, ku, net_h)
+    # then along v for every Bezier row: axis 0 = v
+    pv, vb = _extract_axis0(dv, kv, np.moveaxis(pu, 2, 0))  # (nsv, dv+1, nsu, du+1, 4)
+    patches = np.ascontiguousarray(np.transpose(pv, (2, 0, 3, 1, 4)))  # (nsu, nsv, du+1, dv+1, 4)
+    return patches, ub, vb
 
 
 def elevate_to_cubic(pts_h):

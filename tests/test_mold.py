@@ -1,5 +1,6 @@
-"""The mold cavity (parts.mold): 630 faces, 500 of them one-span B-spline faces of the
-pocket's floor joined along shared B-spline edges, and 40 filleted bosses on the rim.
+"""The mold cavity (parts.mold): 630 faces, 500 of them B-spline faces of 8 x 8 to
+24 x 24 control points (5 to 21 spans a side) cut from the pocket's floor and joined along
+shared B-spline edges, and 40 filleted bosses on the rim.
 
 CPU: the oracle's distances over the rim's material away from the pocket's corners and
 the bosses are the closed form (the nearest of six planes), and over the pocket never
@@ -61,7 +62,7 @@ def test_pocket_against_a_sampled_floor(oracle_mod):
 
     b, o = solid_and_oracle(oracle_mod)
     nets = np.concatenate([p.reshape(-1, 4, 4, 4) for p in b.patches])
-    t = np.linspace(0.0, 1.0, 41)
+    t = np.linspace(0.0, 1.0, 6)  # spans of ~0.6 mm: samples ~0.12 mm apart
     bern = np.stack([(1 - t) ** 3, 3 * t * (1 - t) ** 2, 3 * t ** 2 * (1 - t), t ** 3], 1)
     s = np.einsum("ai,bj,nijk->nabk", bern, bern, nets)
     tree = cKDTree((s[..., :3] / s[..., 3:]).reshape(-1, 3))
@@ -72,7 +73,7 @@ def test_pocket_against_a_sampled_floor(oracle_mod):
     assert (np.abs(d) <= ds + 1e-9).all()
     # above the floor and nearer to it than to any wall (the rim's top and the bosses lie
     # beyond the walls), the floor is the nearest feature: equal within the sampling's
-    # spacing (spans of ~8 mm sampled 40 times, steeper than 1:1 in places: < 0.2 mm)
+    # spacing (spans of ~0.6 mm sampled 5 times, steeper than 1:1 in places: < 0.2 mm)
     x, y = q[:, 0], q[:, 1]
     walls = np.minimum.reduce([x - RIM, X - RIM - x, y - RIM, Y - RIM - y])
     up = (d > 0) & (ds < walls - 0.05)
