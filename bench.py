@@ -532,16 +532,19 @@ def batch_parts(seed0=0, count=64):
 
 def run_batch(args, rank, world):
     """64 uneven parts at h = 0.2 mm, band 1 mm, baked as one batch (one brick launch,
-    a replayed graph, autotuned tiling) and one part at a time; wall time of the
-    synchronous calls (each part's decision is host-driven on its own stream)."""
+    a replayed graph, autotuned tiling) in each arithmetic (FP64, mixed, mixed with the
+    seed network's starts, each part's net trained briefly first), and the headline arm
+    one part at a time; wall time of the synchronous calls. The headline arm's maps and
+    atlases of one part of each family are checked against the f64 oracle."""
     import torch
 
     from implicitcam_b200 import part_gpu
 
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
     h, band = 0.2, 1.0
-    prec = {"fp64": part_gpu.FP64, "mixed": part_gpu.MIXED, "learned": part_gpu.MIXED}[args.precision]
-    gs, levels, faces, fams = [], [], [], []
+    precs = {"fp64": part_gpu.FP64, "mixed": part_gpu.MIXED, "learned": part_gpu.MIXED_LEARNED}
+    prec = precs[args.precision]
+    gs, levels, faces, fams, solids = [], [], [], [], []
     for fam, solid in batch_parts(seed0=64 * rank):
         # certificates for points within the band (a node reads a sub-patch only nearer
         # than the clamp); the brick-wide margin would split these curved tops far deeper
@@ -553,14 +556,31 @@ def run_batch(args, rank, world):
         levels.append((h, lo2, nb, band))
         faces.append(g.info()["faces"])
         fams.append(fam)
-    batch = part_gpu.Batch(gs)
-    for _ in range(args.warmup):
-        batch.bake(levels, precision=prec, read=False)
-    torch.cuda.synchronize()
+        solids.append(solid)
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        st, _ = batch.bake(levels, precision=prec, read=False)
-    t_batch = (time.perf_counter() - t0) / args.steps
+    for i, g in enumerate(gs):  # the seed networks, before any timing (1500 steps of 2048 pairs)
+        if g.info()["subs"] > 0:  # a part without B-spline faces has nothing to seed
+            g.seednet_train(1500, batch=2048, seed=i, need=band)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    batch = part_gpu.Batch(gs)
+
+    def timed(p):
+        for _ in range(args.warmup):
+            batch.bake(levels, precision=p, read=False)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            st, _ = batch.bake(levels, precision=p, read=False)
+        return (time.perf_counter() - t0) / args.steps, st
+
+    arms = {}
+    for name, p in precs.items():
+        t, st = timed(p)
+        arms[name] = {"ms_per_step": 1e3 * t, "value": 512.0 * st["bricks_read"] / t,
+                      "ms_decide": st["ms_decide"], "ms_bricks": st["ms_bricks"], "warps": st["warps"],
+                      "graph_replayed": st["graph_replayed"]}
+    t_batch, st = timed(prec)
     for g, L in zip(gs, levels):  # one part at a time, warm
         g.level_device(*L, precision=prec)
     torch.cuda.synchronize()
@@ -573,6 +593,26 @@ def run_batch(args, rank, world):
                 per_part.append(s1["bricks_read"])
     t_alone = (time.perf_counter() - t0) / args.steps
     voxels = 512.0 * st["bricks_read"]
+    error = None
+    if rank == 0 and not args.no_cpu:
+        # the checker, outside every timed region: one part of each family
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import icam_oracle
+
+        _, res = batch.bake(levels, precision=prec, read=True)
+        error = {}
+        for fam in sorted(set(fams)):
+            i = fams.index(fam)
+            orc = icam_oracle.Oracle(solids[i])
+            hh, lo2, nb, clamp = levels[i]
+            om, _, _ = orc.decide(hh, lo2, nb, clamp)
+            m, a = res[i]
+            r = verify_against_oracle(gs[i], orc, part_gpu, lo2, nb, hh, clamp, prec, m, a, n_bricks=200,
+                                      n_centres=100, decision=om)
+            error[fam] = {k: r[k] for k in ("i16_max_step_diff", "sign_flips", "distance_max_over_diag",
+                                           "decided_entries_differ", "stored_outside_read_set",
+                                           "air_solid_centres_wrong", "nodes_checked") if k in r}
+            error[fam]["part"] = i
     if rank == 0:
         out = {"metric": "batched uneven parts: narrow-band SDF voxels/s", "value": voxels / t_batch,
                "unit": "voxels/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -582,12 +622,15 @@ def run_batch(args, rank, world):
                "config": {"workload": f"64 seeded uneven parts, h={h} mm, band +-{band} mm", "parts": len(gs),
                           "faces_min_max": [min(faces), max(faces)],
                           "bricks_read_min_max": [min(per_part), max(per_part)], "precision": args.precision},
+               "arms": arms, "speedup_vs_fp64": arms["fp64"]["ms_per_step"] / (1e3 * t_batch),
+               "seednet_train_s": train_s,
                "one_part_at_a_time": {"value": voxels / t_alone, "ms_per_step": 1e3 * t_alone},
                "speedup_vs_one_at_a_time": t_alone / t_batch,
                "families": {fam: {"parts": fams.count(fam),
                                   "faces": sum(n for n, f in zip(faces, fams) if f == fam),
                                   "bricks_read": sum(n for n, f in zip(per_part, fams) if f == fam)}
                             for fam in sorted(set(fams))},
+               "error_vs_oracle": error,
                "batch_stats": {k: st[k] for k in ("bricks_read", "bricks_words", "warps", "graph_replayed",
                                                   "tune_ms", "ms_decide", "ms_bricks", "kernel_launches")}}
         print(json.dumps(out), flush=True)

@@ -65,6 +65,7 @@ int scratch(IcamPack* pk, int k, size_t bytes, void** out) {
 // trained or loaded on this pack).
 int learned_starts(IcamPack* pk, int precision, BrickArgs* a) {
   if (precision != ICAM_MIXED_LEARNED) return ICAM_OK;
+  if (pk->dev.n_subs == 0) return ICAM_OK;  // no B-spline sub-patch to seed: ICAM_MIXED
   if (!pk->net.ready)
     return fail(pk, ICAM_ERR_ARG, "ICAM_MIXED_LEARNED: train (icam_seednet_train) or load the seed network first");
   a->net_feat = pk->net.feat;
@@ -804,7 +805,7 @@ extern "C" int icam_bricks_static(IcamPack* pk, const double* first_nodes, size_
   if (pk->device < 0 || pk->device >= kStaticDevices)
     return static_fail(err, errlen, ICAM_ERR_ARG, "device ordinal out of range", nullptr);
   // ICAM_MIXED_LEARNED needs the pack's trained seed network, as icam_bricks does
-  if (precision == ICAM_MIXED_LEARNED && !pk->net.ready)
+  if (precision == ICAM_MIXED_LEARNED && !pk->net.ready && pk->dev.n_subs > 0)
     return static_fail(err, errlen, ICAM_ERR_ARG,
                        "ICAM_MIXED_LEARNED: train (icam_seednet_train) or load the seed network first", nullptr);
   if (n == 0) return ICAM_OK;
@@ -834,7 +835,7 @@ extern "C" int icam_bricks_static(IcamPack* pk, const double* first_nodes, size_
   a.leaves = pk->leaves;
   a.n_leaves = int32_t(pk->leaves_host.size());
   a.mixed = precision != ICAM_FP64;
-  if (precision == ICAM_MIXED_LEARNED) {  // the starts the seed network puts, as icam_bricks takes them
+  if (precision == ICAM_MIXED_LEARNED && pk->dev.n_subs > 0) {  // the seed network's starts, as icam_bricks takes them
     a.net_feat = pk->net.feat;
     a.net_w = pk->net.wbf;
   }

@@ -238,7 +238,7 @@ int icam_batch_bake(IcamBatch* bt, const IcamBatchLevel* levels, int precision, 
       cleanup();
       return bfail(bt, ICAM_ERR_ARG, "part " + std::to_string(i) + ": level too large");
     }
-    if (precision == ICAM_MIXED_LEARNED && !pk->net.ready) {
+    if (precision == ICAM_MIXED_LEARNED && !pk->net.ready && pk->dev.n_subs > 0) {
       cleanup();
       return bfail(bt, ICAM_ERR_ARG, "ICAM_MIXED_LEARNED: part " + std::to_string(i) + " has no trained seed network");
     }
@@ -393,7 +393,7 @@ int icam_batch_bake(IcamBatch* bt, const IcamBatchLevel* levels, int precision, 
     q.n_leaves = int32_t(pk->leaves_host.size());
     q.h = lv.h;
     q.clamp = lv.clamp;
-    if (precision == ICAM_MIXED_LEARNED) q.net_feat = pk->net.feat, q.net_w = pk->net.wbf;
+    if (precision == ICAM_MIXED_LEARNED && pk->dev.n_subs > 0) q.net_feat = pk->net.feat, q.net_w = pk->net.wbf;
   }
   BCK(cudaMemcpyAsync(bt->d_parts, hp.data(), n * sizeof(PartParams), cudaMemcpyHostToDevice, s));
   BCK(cudaMemcpyAsync(d_maps, maps.data(), n * sizeof(uint32_t*), cudaMemcpyHostToDevice, s));

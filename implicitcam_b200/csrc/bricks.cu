@@ -37,7 +37,6 @@ struct BrickSmem {
   int n;
 };
 static_assert(sizeof(BrickSmem) * MAX_WARPS <= 48 * 1024, "shared memory of a block");
-static_assert(sizeof(((BrickSmem*)0)->u) >= 32 * SN_KS * 2 + 32 * 8 * 4, "the seed network's room in the list's");
 
 // One brick a warp:
 //  0. a brick whose centre distance puts every node past the clamp is written at once;
@@ -77,8 +76,6 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 2) k_bricks_t(BrickArgs a) {
     const double h = BATCH ? Q->h : a.h, clamp = BATCH ? Q->clamp : a.clamp;
     const int32_t* leaves = BATCH ? Q->leaves : a.leaves;
     const int32_t n_leaves = BATCH ? Q->n_leaves : a.n_leaves;
-    const float* net_feat = BATCH ? Q->net_feat : a.net_feat;
-    const void* net_w = BATCH ? Q->net_w : a.net_w;
     double3 first = mk(a.firsts[3 * bi], a.firsts[3 * bi + 1], a.firsts[3 * bi + 2]);
     const double half = 4.0 * h;
     const double3 c = first + mk(half, half, half);
@@ -134,18 +131,7 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 2) k_bricks_t(BrickArgs a) {
         const unsigned m = __ballot_sync(FULL, is_sub);
         const int before = subs_before + __popc(m & ((1u << lane) - 1u));
         subs_before += __popc(m);
-        // MIXED_LEARNED: the centre solves start where the seed network puts them, its 32
-        // queries (this group of candidates at the centre) on the tensor cores, in the
-        // room of the list, which is ranked by now
-        double s0 = 0.5, t0 = 0.5;
-        if (net_w) {
-          float x[SN_IN], y[3];
-          const int fi = is_sub ? int(S.code[k] & IK_MASK) : 0;
-          sn_input(net_feat + size_t(fi) * SN_FEAT, c, x);
-          __nv_bfloat16* act = reinterpret_cast<__nv_bfloat16*>(&S.u);
-          sn_forward_warp(net_w, act, reinterpret_cast<float*>(act + 32 * SN_KS), x, y, lane);
-          s0 = fmin(fmax(double(y[0]), 0.0), 1.0), t0 = fmin(fmax(double(y[1]), 0.0), 1.0);
-        }
+        const double s0 = 0.5, t0 = 0.5;  // the plain form starts at the sub-patch's centre
         if (k >= n) continue;
         int slot = -1;
         int8_t cert = 0;

@@ -15,6 +15,11 @@ constexpr int8_t FS_PENDING = 2, FS_AIR = 3, FS_SOLID = -3;
 // A box group's list holds twice a brick's candidates: a box's cut reaches farther, and
 // a list that overflows sends every lane to walk the tree alone.
 constexpr int DMAXC = 2 * MAXC;
+// A group whose list overflows is halved (each half lists again) while the list holds
+// fewer than HALVE_BELOW times the room; past that (a part of many small faces, where
+// even one box's cut holds far more than the room) halving would end in boxes walking
+// the tree one lane at a time, so the group's lanes walk it each for its own box at once.
+constexpr int HALVE_BELOW = 16;
 
 struct DecideSmem {
   uint32_t tcode[DMAXC];  // the list before its ranking, and the walk's frontier
@@ -181,13 +186,13 @@ __device__ __forceinline__ void decide_group(const DecideArgs& a, const Box4* bo
     double R, bl[3], bh[3];
     centres_ball(c, mine, l0, lane, &gc, &R, bl, bh);
     // every feature nearer than the cut to a centre has a bound <= R + cut from gc
-    int nc = warp_list<DMAXC>(P, a.leaves, a.n_leaves, gc, R + cut, S.tcode, S.tlb, S.fr, &S.n, lane);
+    int nc = warp_list<DMAXC, true>(P, a.leaves, a.n_leaves, gc, R + cut, S.tcode, S.tlb, S.fr, &S.n, lane);
     const bool overflow = nc > DMAXC;
-    if (overflow && sg > 1) {
+    if (overflow && sg > 1 && nc < HALVE_BELOW * DMAXC) {
       sg = (sg + 1) / 2;
       continue;
     }
-    if (overflow) nc = DMAXC;
+    if (overflow) nc = 0;  // the points walk the tree: the list is not read (nor complete)
     warp_rank(S.tcode, S.tlb, nc, S.code, S.lb, lane);
     int subs_before = 0;
     for (int base = 0; base < nc; base += 32) {
@@ -297,14 +302,14 @@ __device__ __forceinline__ void decide_group_f(const DecideArgs& a, const Box4* 
     double3 gc;
     double R, bl[3], bh[3];
     centres_ball(c, mine, l0, lane, &gc, &R, bl, bh);
-    int nc = warp_list<DMAXC>(P, a.leaves, a.n_leaves, gc, R + cut, S.u.list.tcode, S.u.list.tlb, S.u.list.fr, &S.n,
+    int nc = warp_list<DMAXC, true>(P, a.leaves, a.n_leaves, gc, R + cut, S.u.list.tcode, S.u.list.tlb, S.u.list.fr, &S.n,
                               lane);
     const bool overflow = nc > DMAXC;
-    if (overflow && sg > 1) {
+    if (overflow && sg > 1 && nc < HALVE_BELOW * DMAXC) {
       sg = (sg + 1) / 2;
       continue;
     }
-    if (overflow) nc = DMAXC;
+    if (overflow) nc = 0;  // the points walk the tree: the list is not read (nor complete)
     warp_rank(S.u.list.tcode, S.u.list.tlb, nc, S.code, S.lb, lane);
     const double3 blo = mk(bl[0], bl[1], bl[2]), bhi = mk(bh[0], bh[1], bh[2]);
     int subs_before = 0;

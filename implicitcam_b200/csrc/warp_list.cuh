@@ -10,14 +10,17 @@ namespace icam {
 
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int MAXC = 128;   // candidates a list may hold
-constexpr int FR = 64;      // tree nodes one level of the list's walk may hold
+constexpr int FR = 128;     // tree nodes one level of the list's walk may hold
 constexpr int MAXSUB = 32;  // sub-patches seeded from the centre
 
 // The features with a lower bound <= reach from c, unranked into tcode / tlb (at most
 // CAP kept; the count returned may exceed it). The tree is walked a level at a time,
-// a lane a node; a level wider than the frontier gives way to every leaf in turn.
+// a lane a node; a level wider than the frontier gives way to every leaf in turn, or,
+// with WIDE_GIVES_UP, ends the walk with a count of LIST_TOO_WIDE (more than any room:
+// the caller reads its points by the tree walk instead).
 // *count is a shared counter of the warp; fr two frontier buffers of FR nodes.
-template <int CAP = MAXC>
+constexpr int LIST_TOO_WIDE = 1 << 28;
+template <int CAP = MAXC, bool WIDE_GIVES_UP = false>
 __device__ __forceinline__ int warp_list(const DPack& P, const int32_t* leaves, int n_leaves, double3 c, double reach,
                                          uint32_t* tcode, double* tlb, int32_t (*fr)[FR], int* count, int lane) {
   auto take_leaf = [&](const DBvh& nd) {
@@ -72,6 +75,10 @@ __device__ __forceinline__ int warp_list(const DPack& P, const int32_t* leaves, 
     }
     cur ^= 1;
     ncur = nnext;
+  }
+  if (!walked && WIDE_GIVES_UP) {
+    __syncwarp();
+    return LIST_TOO_WIDE;
   }
   if (!walked) {
     if (lane == 0) *count = 0;

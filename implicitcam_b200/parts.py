@@ -649,7 +649,8 @@ def mold(seed=0, size=(250.0, 200.0, 80.0), rim=25.0, fu=25, fv=20, floor=40.0, 
          spans=(5, 21)):
     """A mold cavity: a size block with a pocket `rim` mm in from its sides, the pocket's
     floor one clamped bicubic rational B-spline (heights floor plus `bumps` seeded
-    Gaussians, amplitude U[2,8] mm, sigma U[10,40] mm; weights U[0.8,1.2]; uniform knots)
+    Gaussians, amplitude U[2,8] mm, sigma U[10,40] mm; weights in [0.8, 1.2] from three
+    seeded plane waves of 30-90 mm; uniform knots)
     cut along its knot lines into fu x fv faces: face column a holds m_u[a] spans, face row
     c m_v[c], each drawn from `spans`, so a face is a patch of (m_u + 3) x (m_v + 3)
     control points (8 x 8 to 24 x 24) and neighbouring faces join C2 along shared B-spline
@@ -670,7 +671,11 @@ def mold(seed=0, size=(250.0, 200.0, 80.0), rim=25.0, fu=25, fv=20, floor=40.0, 
     ys = ay + (by - ay) * np.arange(nv) / (nv - 1)
     XX, YY = np.meshgrid(xs, ys, indexing="ij")
     zz = floor + sum(a * np.exp(-((XX - cx) ** 2 + (YY - cy) ** 2) / (2 * s * s)) for a, s, cx, cy in g)
-    w = np.array([rng.uniform(0.8, 1.2) for _ in range(nu * nv)]).reshape(nu, nv)
+    # weights in [0.8, 1.2] from a seeded field over the floor (three plane waves of 30 to
+    # 90 mm), not drawn a control point at a time: on a net of control points a fraction
+    # of a millimetre apart, independent weights would ripple the surface at that scale
+    waves = [(rng.uniform(30.0, 90.0), rng.uniform(0.0, TAU), rng.uniform(0.0, TAU)) for _ in range(3)]
+    w = 1.0 + 0.2 / 3.0 * sum(np.cos(TAU / L * (XX * math.cos(a) + YY * math.sin(a)) + ph) for L, a, ph in waves)
     net = np.stack([XX * w, YY * w, zz * w, w], -1)
     ku = [0.0] * 4 + [k / su for k in range(1, su)] + [1.0] * 4
     kv = [0.0] * 4 + [k / sv for k in range(1, sv)] + [1.0] * 4

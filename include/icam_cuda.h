@@ -41,7 +41,8 @@ extern "C" {
 enum {
   ICAM_FP64 = 0,          /* every step in double precision */
   ICAM_MIXED = 1,         /* single-precision bulk, double-precision polish, trim near loops and signs */
-  ICAM_MIXED_LEARNED = 2  /* ICAM_MIXED seeded by the pack's trained seed network */
+  ICAM_MIXED_LEARNED = 2  /* ICAM_MIXED seeded by the pack's trained seed network (a solid with no
+                             B-spline sub-patch has nothing to seed: ICAM_MIXED) */
 };
 
 /* Status codes. */
