@@ -49,6 +49,52 @@ struct SpanGrid {
   std::vector<Bicubic> spans;
   int nsu, nsv;
 };
+// Whether a B-spline face's spans meet without a crease and none of its sides collapses
+// to a point: the unit normals on either side of every interior span boundary agree (a
+// crease is an interior knot line where the surface is only C0, Exact::c0_line,
+// solid3.rs:1821), and the normal is defined along every span side (a side collapsed to
+// one point is a pole, solid3.rs:1609-1625). This pack builds neither feature, so a face
+// with one is refused rather than packed with its nearest points on the crease or at the
+// pole missing.
+bool spans_smooth(const SpanGrid& g, std::string* why) {
+  auto normal = [](const Bicubic& sp, double s, double t, double* len) {
+    V P, Ps, Pt, Pss, Pst, Ptt;
+    sp.eval(s, t, &P, &Ps, &Pt, &Pss, &Pst, &Ptt);
+    V n = Ps.cross(Pt);
+    *len = n.len() / std::max(Ps.len() * Pt.len(), 1e-300);
+    return n.unit();
+  };
+  const double ts[5] = {0.0, 0.25, 0.5, 0.75, 1.0};
+  for (int a = 0; a < g.nsu; a++)
+    for (int b = 0; b < g.nsv; b++) {
+      const Bicubic& sp = g.spans[a * g.nsv + b];
+      for (double t : ts)
+        for (int side = 0; side < 4; side++) {
+          const double s0 = side == 0 ? 0.0 : (side == 1 ? 1.0 : t), t0 = side == 2 ? 0.0 : (side == 3 ? 1.0 : t);
+          double l;
+          normal(sp, s0, t0, &l);
+          if (!(l > 1e-9)) {
+            *why = "a side of its B-spline surface collapses to a point (a pole): not packed";
+            return false;
+          }
+        }
+      for (int k = 0; k < 2; k++) {  // the boundary to the next span along u (k 0) or v (k 1)
+        if ((k == 0 && a + 1 >= g.nsu) || (k == 1 && b + 1 >= g.nsv)) continue;
+        const Bicubic& nx = g.spans[k == 0 ? (a + 1) * g.nsv + b : a * g.nsv + b + 1];
+        for (double t : ts) {
+          double l0, l1;
+          const V n0 = k == 0 ? normal(sp, 1.0, t, &l0) : normal(sp, t, 1.0, &l0);
+          const V n1 = k == 0 ? normal(nx, 0.0, t, &l1) : normal(nx, t, 0.0, &l1);
+          if ((n0 - n1).len() > 1e-7) {
+            *why = "its B-spline surface has a crease along an interior knot line (C0): not packed";
+            return false;
+          }
+        }
+      }
+    }
+  return true;
+}
+
 void nearest_on(const SpanGrid& g, V x, double* u, double* v, V* n, double* dist) {
   double best = 1e300;
   for (auto& sp : g.spans) {
@@ -198,6 +244,11 @@ bool build_pack(const IcamSolidDesc* d, double need, HostPack* hp, std::string* 
               P.span_cp.push_back({h[0], h[1], h[2], h[3]});
             }
         }
+      std::string why;
+      if (!spans_smooth(grids[fi], &why)) {
+        *err = "face " + std::to_string(fi) + ": " + why;
+        return false;
+      }
       f.nurbs = int(P.nurbs.size());
       P.nurbs.push_back(nb);
     } else if (fd.kind < 0 || fd.kind > 4) {

@@ -64,3 +64,33 @@ def test_rust_binding_names_match_the_header():
     text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
     rust = sorted(set(re.findall(r"pub fn (icam_\w+)\(", text)))
     assert rust == declared()
+
+
+def test_a_creased_bspline_face_is_refused():
+    """A B-spline face with a C0 crease along an interior knot line (a triple knot of a
+    cubic whose control heights fold there) is refused when packed, before any device
+    work: the pack has no knot-line features (Exact::c0_line), so it must not bake such
+    a face with the crease's nearest points missing. The same top without the fold packs."""
+    import numpy as np
+
+    from implicitcam_b200 import part_gpu, parts
+    from implicitcam_b200.solid import SolidBuilder
+
+    def top(fold):
+        n, size = 7, 30.0
+        net = np.zeros((n, n, 4))
+        for i in range(n):
+            for j in range(n):
+                x, y = size * i / (n - 1), size * j / (n - 1)
+                z = 10.0 + (fold * abs(x - size / 2) if fold else 0.02 * x * y / size)
+                net[i, j] = [x, y, z, 1.0]
+        knots = [0.0] * 4 + [0.5] * 3 + [1.0] * 4
+        return parts._nurbs_box(SolidBuilder(tol=1e-9), 3, 3, knots, knots, net, size, size)
+
+    with pytest.raises(part_gpu.IcamError, match="crease"):
+        part_gpu.PartGpu(top(0.3))
+    # the unfolded top passes the check (it may then fail only for want of a GPU)
+    try:
+        part_gpu.PartGpu(top(0.0)).close()
+    except part_gpu.IcamError as e:
+        assert "crease" not in str(e) and "pole" not in str(e)
