@@ -89,6 +89,25 @@ def newton_figures(st):
             "nodes_double": st.get("nodes_double", 0), "centres_double": st.get("centres_double", 0)}
 
 
+# FLOPs of one float patch evaluation and Newton step (eval_bicubic_f: the rows' and
+# columns' Bernstein sums of the point and its first and second derivatives, ~600; the
+# rational quotients, ~50; the 2 x 2 Newton step, ~50)
+FLOPS_PER_FLOAT_EVAL = 700.0
+
+
+def executed_roofline(st, node_ms, peak):
+    """The work the mixed walk did in the bake: its float patch evaluations (counted by
+    the kernel) at FLOPS_PER_FLOAT_EVAL each, over the node phase's time, against the
+    FP32 probe (None for the FP64 arm, whose evaluations are not counted)."""
+    ev = st.get("newton_evals", 0)
+    if not ev:
+        return None
+    f = FLOPS_PER_FLOAT_EVAL * ev
+    return {"flops_per_launch": f, "achieved": f / (node_ms * 1e-3) / 1e12, "unit": "TFLOP/s",
+            "frac": f / (node_ms * 1e-3) / peak,
+            "note": "float patch evaluations the kernel counted x 700 FLOPs, over the node phase"}
+
+
 def over_ranks(dist, device, ms, voxels=None):
     """The job's figures over the ranks: the slowest rank's time (max) and every rank's
     voxels (sum); as given on one process. Every rank calls it at the same point."""
@@ -403,7 +422,8 @@ def main():
                          "frac": achieved / peak, "traffic": TRAFFIC_PER_READ_BRICK * st["bricks_read"],
                          "traffic_source": "ncu dram bytes of k_bricks at h = 0.2 mm, scaled by bricks read",
                          "peak_source": "measured FMA probe of this run (MEASURED_PEAKS.json holds no FP64/FP32 figure)",
-                         "algorithmic_flops_per_launch": flops},
+                         "algorithmic_flops_per_launch": flops,
+                         "executed": executed_roofline(st, node_ms, peak)},
             "cpu_baseline": cpu,
             "clocks": clocks,
         }

@@ -61,7 +61,7 @@ struct DSub {
 };
 
 struct DEdge {
-  int32_t kind;  // 0 line, 1 arc, 2 spline
+  int32_t kind;  // 0 line, 1 arc, 2 spline, 3 a crease of face f0 (= f1) inside it
   int32_t f0, f1;
   int32_t first_piece, n_pieces;
   int32_t pad;

@@ -49,14 +49,15 @@ struct SpanGrid {
   std::vector<Bicubic> spans;
   int nsu, nsv;
 };
-// Whether a B-spline face's spans meet without a crease and none of its sides collapses
-// to a point: the unit normals on either side of every interior span boundary agree (a
-// crease is an interior knot line where the surface is only C0, Exact::c0_line,
-// solid3.rs:1821), and the normal is defined along every span side (a side collapsed to
-// one point is a pole, solid3.rs:1609-1625). This pack builds neither feature, so a face
-// with one is refused rather than packed with its nearest points on the crease or at the
-// pole missing.
-bool spans_smooth(const SpanGrid& g, std::string* why) {
+// A B-spline face's creases: the interior span boundaries across which the spans' unit
+// normals differ (sampled at five points a span; 1e-7), where the surface is only C0 and
+// folds (Exact::c0_line, solid3.rs:1821; the reference finds them by knots of full
+// multiplicity, a knot line with a continuous normal needs no feature of its own). Each
+// (k, a): the boundary before span a along u (k 0) or v (k 1). False, with the reason,
+// when a side of a span collapses to a point (a pole, solid3.rs:1609-1625): this pack
+// has no pole feature, so such a face is refused rather than packed with the pole's
+// nearest points missing.
+bool span_creases(const SpanGrid& g, std::vector<std::pair<int, int>>* creases, std::string* why) {
   auto normal = [](const Bicubic& sp, double s, double t, double* len) {
     V P, Ps, Pt, Pss, Pst, Ptt;
     sp.eval(s, t, &P, &Ps, &Pt, &Pss, &Pst, &Ptt);
@@ -65,34 +66,84 @@ bool spans_smooth(const SpanGrid& g, std::string* why) {
     return n.unit();
   };
   const double ts[5] = {0.0, 0.25, 0.5, 0.75, 1.0};
-  for (int a = 0; a < g.nsu; a++)
-    for (int b = 0; b < g.nsv; b++) {
-      const Bicubic& sp = g.spans[a * g.nsv + b];
-      for (double t : ts)
-        for (int side = 0; side < 4; side++) {
-          const double s0 = side == 0 ? 0.0 : (side == 1 ? 1.0 : t), t0 = side == 2 ? 0.0 : (side == 3 ? 1.0 : t);
-          double l;
-          normal(sp, s0, t0, &l);
-          if (!(l > 1e-9)) {
-            *why = "a side of its B-spline surface collapses to a point (a pole): not packed";
-            return false;
-          }
-        }
-      for (int k = 0; k < 2; k++) {  // the boundary to the next span along u (k 0) or v (k 1)
-        if ((k == 0 && a + 1 >= g.nsu) || (k == 1 && b + 1 >= g.nsv)) continue;
-        const Bicubic& nx = g.spans[k == 0 ? (a + 1) * g.nsv + b : a * g.nsv + b + 1];
-        for (double t : ts) {
-          double l0, l1;
-          const V n0 = k == 0 ? normal(sp, 1.0, t, &l0) : normal(sp, t, 1.0, &l0);
-          const V n1 = k == 0 ? normal(nx, 0.0, t, &l1) : normal(nx, t, 0.0, &l1);
-          if ((n0 - n1).len() > 1e-7) {
-            *why = "its B-spline surface has a crease along an interior knot line (C0): not packed";
-            return false;
-          }
+  for (auto& sp : g.spans)
+    for (double t : ts)
+      for (int side = 0; side < 4; side++) {
+        const double s0 = side == 0 ? 0.0 : (side == 1 ? 1.0 : t), t0 = side == 2 ? 0.0 : (side == 3 ? 1.0 : t);
+        double l;
+        normal(sp, s0, t0, &l);
+        if (!(l > 1e-9)) {
+          *why = "a side of its B-spline surface collapses to a point (a pole): not packed";
+          return false;
         }
       }
+  for (int k = 0; k < 2; k++) {
+    const int na = k == 0 ? g.nsu : g.nsv, nb = k == 0 ? g.nsv : g.nsu;
+    for (int a = 1; a < na; a++) {
+      bool crease = false;
+      for (int b = 0; b < nb && !crease; b++) {
+        const Bicubic& p0 = g.spans[k == 0 ? (a - 1) * g.nsv + b : b * g.nsv + a - 1];
+        const Bicubic& p1 = g.spans[k == 0 ? a * g.nsv + b : b * g.nsv + a];
+        for (double t : ts) {
+          double l0, l1;
+          const V n0 = k == 0 ? normal(p0, 1.0, t, &l0) : normal(p0, t, 1.0, &l0);
+          const V n1 = k == 0 ? normal(p1, 0.0, t, &l1) : normal(p1, t, 0.0, &l1);
+          if ((n0 - n1).len() > 1e-7) crease = true;
+        }
+      }
+      if (crease) creases->push_back({k, a});
     }
+  }
   return true;
+}
+
+// A rational cubic with its parameter range on the curve it was cut from.
+struct CutPiece {
+  Cubic3 z;
+  double t0, t1;
+};
+
+// A spline curve's pieces made flat (split until the control polygon turns <= 0.35,
+// curve3.rs:1017-1031), then each halved (up to 5 times) until |C - p|^2 certifies
+// convex for every p within `need` of it, so that points that near take one Newton
+// solve instead of the subdivision search; the curve and its closest points are the
+// same, the halves' ends only add points of it to try.
+std::vector<CutPiece> flat_pieces(const std::vector<CutPiece>& in, double need) {
+  std::vector<CutPiece> flat, stack(in.rbegin(), in.rend());
+  while (!stack.empty()) {
+    CutPiece q = stack.back();
+    stack.pop_back();
+    if (q.z.turning() <= 0.35 || flat.size() > 100000) {
+      flat.push_back(q);
+    } else {
+      CutPiece l, r;
+      q.z.split(0.5, &l.z, &r.z);
+      const double m = 0.5 * (q.t0 + q.t1);
+      l.t0 = q.t0, l.t1 = m, r.t0 = m, r.t1 = q.t1;
+      stack.push_back(r);
+      stack.push_back(l);
+    }
+  }
+  std::vector<CutPiece> fine;
+  std::vector<std::pair<CutPiece, int>> st;
+  for (const CutPiece& z0 : flat) {
+    st.assign(1, {z0, 0});
+    while (!st.empty()) {
+      auto q = st.back();
+      st.pop_back();
+      if (q.second >= 5 || piece_certifies(q.first.z, need)) {
+        fine.push_back(q.first);
+      } else {
+        CutPiece l, r;
+        q.first.z.split(0.5, &l.z, &r.z);
+        const double m = 0.5 * (q.first.t0 + q.first.t1);
+        l.t0 = q.first.t0, l.t1 = m, r.t0 = m, r.t1 = q.first.t1;
+        st.push_back({r, q.second + 1});
+        st.push_back({l, q.second + 1});
+      }
+    }
+  }
+  return fine;
 }
 
 void nearest_on(const SpanGrid& g, V x, double* u, double* v, V* n, double* dist) {
@@ -178,6 +229,7 @@ bool build_pack(const IcamSolidDesc* d, double need, HostPack* hp, std::string* 
   }
   // ---------------------------------------------------------------- faces and spans
   std::vector<SpanGrid> grids(d->n_faces);
+  std::vector<std::vector<std::pair<int, int>>> creases(d->n_faces);
   std::vector<TrimTree> trees(d->n_faces);
   for (int fi = 0; fi < d->n_faces; fi++) {
     const IcamFaceDesc& fd = d->faces[fi];
@@ -245,7 +297,7 @@ bool build_pack(const IcamSolidDesc* d, double need, HostPack* hp, std::string* 
             }
         }
       std::string why;
-      if (!spans_smooth(grids[fi], &why)) {
+      if (!span_creases(grids[fi], &creases[fi], &why)) {
         *err = "face " + std::to_string(fi) + ": " + why;
         return false;
       }
@@ -335,56 +387,20 @@ bool build_pack(const IcamSolidDesc* d, double need, HostPack* hp, std::string* 
         *err = "edge " + std::to_string(ei) + ": spline degrees above 3 are not packed";
         return false;
       }
-      // flat pieces (curve3.rs:1017-1031: split until the control polygon turns <= 0.35)
-      std::vector<Cubic3> flat, stack;
-      for (int k = ed.n_pieces - 1; k >= 0; k--) {
+      std::vector<CutPiece> cut;
+      for (int k = 0; k < ed.n_pieces; k++) {
         const double* c = d->cpieces + size_t(ed.first_piece + k) * (ed.degree + 1) * 4;
         std::vector<H> q;
         for (int j = 0; j <= ed.degree; j++) q.push_back({c[4 * j], c[4 * j + 1], c[4 * j + 2], c[4 * j + 3]});
         while (q.size() < 4) q = elevate(q);
-        Cubic3 z;
-        for (int j = 0; j < 4; j++) z.c[j] = q[j];
-        stack.push_back(z);
+        CutPiece z;
+        for (int j = 0; j < 4; j++) z.z.c[j] = q[j];
+        z.t0 = k, z.t1 = k + 1;
+        cut.push_back(z);
       }
-      while (!stack.empty()) {
-        Cubic3 z = stack.back();
-        stack.pop_back();
-        if (z.turning() <= 0.35 || flat.size() > 100000) {
-          flat.push_back(z);
-        } else {
-          Cubic3 l, r;
-          z.split(0.5, &l, &r);
-          stack.push_back(r);
-          stack.push_back(l);
-        }
-      }
-      // each flat piece halved (up to 5 times) until |C - p|^2 certifies convex for
-      // every p within `need` of it, so that points that near take one Newton solve
-      // instead of the subdivision search; the curve and its closest points are the
-      // same, the halves' ends only add points of it to try
-      {
-        std::vector<Cubic3> fine;
-        struct Part {
-          Cubic3 z;
-          int depth;
-        };
-        for (const Cubic3& z0 : flat) {
-          std::vector<Part> st{{z0, 0}};
-          while (!st.empty()) {
-            Part q = st.back();
-            st.pop_back();
-            if (q.depth >= 5 || piece_certifies(q.z, need)) {
-              fine.push_back(q.z);
-            } else {
-              Cubic3 l, r;
-              q.z.split(0.5, &l, &r);
-              st.push_back({r, q.depth + 1});
-              st.push_back({l, q.depth + 1});
-            }
-          }
-        }
-        flat.swap(fine);
-      }
+      std::vector<CutPiece> fp = flat_pieces(cut, need);
+      std::vector<Cubic3> flat;
+      for (auto& q : fp) flat.push_back(q.z);
       e.first_piece = int(P.pieces.size());
       e.n_pieces = int(flat.size());
       for (size_t k = 0; k < flat.size(); k++) {
@@ -430,6 +446,79 @@ bool build_pack(const IcamSolidDesc* d, double need, HostPack* hp, std::string* 
       }
     for (int c = 0; c < 3; c++) e.box[c] = box.lo[c], e.box[3 + c] = box.hi[c];
     P.edges.push_back(e);
+  }
+  // ---------------------------------------------------------------- creases (solid3.rs:1821-1886)
+  // A B-spline face's crease as an edge of that face with itself: its pieces are the
+  // iso-curve on the knot line (the side of the span after it), flat and certified as a
+  // spline edge's; each piece keeps the parameters of its ends on either side, nudged a
+  // billionth of a span into the span before the line for side 0, so that the normals
+  // summed for its sign are the two spans' (the span before at its far side, the span
+  // after at its near side); its first and last pieces' outer ends are where the line
+  // meets the face's boundary, which the boundary's edges answer. A crease must lie
+  // wholly inside its face's loops (the device does not test a crease's feet against
+  // them); one crossing them is refused.
+  for (int fi = 0; fi < d->n_faces; fi++) {
+    if (creases[fi].empty()) continue;
+    const SpanGrid& g = grids[fi];
+    const DNurbs& nbr = P.nurbs[P.faces[fi].nurbs];
+    const double* ubr = P.breaks.data() + nbr.first_break;
+    const double* vbr = ubr + g.nsu + 1;
+    for (auto [k, a] : creases[fi]) {
+      const double value = k == 0 ? ubr[a] : vbr[a];
+      const double* other = k == 0 ? vbr : ubr;
+      const int no = k == 0 ? g.nsv : g.nsu;
+      const double eo = 1e-9 * (other[no] - other[0]);
+      double lo[2], hi[2];
+      lo[k] = hi[k] = value;
+      lo[1 - k] = other[0] + eo;
+      hi[1 - k] = other[no] - eo;
+      if (trees[fi].box_class(lo, hi) != 1) {
+        *err = "face " + std::to_string(fi) + ": a crease that crosses its face's loops is not packed";
+        return false;
+      }
+      std::vector<CutPiece> cut;
+      for (int b = 0; b < no; b++) {
+        const Bicubic& sp = g.spans[k == 0 ? a * g.nsv + b : b * g.nsv + a];
+        CutPiece z;
+        for (int j = 0; j < 4; j++) z.z.c[j] = k == 0 ? sp.p[0][j] : sp.p[j][0];
+        z.t0 = other[b], z.t1 = other[b + 1];
+        cut.push_back(z);
+      }
+      std::vector<CutPiece> fp = flat_pieces(cut, need);
+      const double span_w = k == 0 ? ubr[a] - ubr[a - 1] : vbr[a] - vbr[a - 1];
+      DEdge e{};
+      e.kind = 3;  // a crease
+      e.f0 = e.f1 = fi;
+      e.first_piece = int(P.pieces.size());
+      e.n_pieces = int(fp.size());
+      Bx box;
+      for (size_t q = 0; q < fp.size(); q++) {
+        DPiece pc{};
+        pc.edge = int(P.edges.size());
+        pc.first = q == 0;
+        pc.last = q + 1 == fp.size();
+        for (int j = 0; j < 4; j++)
+          for (int c = 0; c < 4; c++) pc.cp[j][c] = fp[q].z.c[j][c];
+        Bx pb = fp[q].z.box();
+        for (int c = 0; c < 3; c++) pc.box[c] = pb.lo[c], pc.box[3 + c] = pb.hi[c];
+        box.add(pb);
+        pc.thick = fp[q].z.thickness();
+        if (!piece_bounds(fp[q].z.c, &pc.lam, pc.d2)) {
+          *err = "face " + std::to_string(fi) + ": a weight of a crease is not positive";
+          return false;
+        }
+        for (int side = 0; side < 2; side++)
+          for (int end = 0; end < 2; end++) {
+            const double held = side == 0 ? value - 1e-9 * span_w : value;
+            const double along = end == 0 ? fp[q].t0 : fp[q].t1;
+            pc.uv[side][end][k] = held;
+            pc.uv[side][end][1 - k] = along;
+          }
+        P.pieces.push_back(pc);
+      }
+      for (int c = 0; c < 3; c++) e.box[c] = box.lo[c], e.box[3 + c] = box.hi[c];
+      P.edges.push_back(e);
+    }
   }
   // ---------------------------------------------------------------- face boxes (solid3.rs:1211-1278)
   for (int fi = 0; fi < d->n_faces; fi++) {
@@ -589,7 +678,7 @@ bool build_pack(const IcamSolidDesc* d, double need, HostPack* hp, std::string* 
     if (P.faces[i].kind != S_NURBS) items.push_back({(uint32_t(IK_FACE) << IK_SHIFT) | uint32_t(i), box6(P.faces[i].box)});
   for (int i = 0; i < int(P.subs.size()); i++) items.push_back({(uint32_t(IK_SUB) << IK_SHIFT) | uint32_t(i), box6(P.subs[i].box)});
   for (int i = 0; i < int(P.edges.size()); i++)
-    if (P.edges[i].kind != 2) items.push_back({(uint32_t(IK_EDGE) << IK_SHIFT) | uint32_t(i), box6(P.edges[i].box)});
+    if (P.edges[i].kind <= 1) items.push_back({(uint32_t(IK_EDGE) << IK_SHIFT) | uint32_t(i), box6(P.edges[i].box)});
   for (int i = 0; i < int(P.pieces.size()); i++) items.push_back({(uint32_t(IK_PIECE) << IK_SHIFT) | uint32_t(i), box6(P.pieces[i].box)});
   for (int i = 0; i < int(P.verts.size()); i++) {
     Bx b;

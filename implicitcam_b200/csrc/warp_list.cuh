@@ -10,16 +10,18 @@ namespace icam {
 
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int MAXC = 128;   // candidates a list may hold
-constexpr int FR = 128;     // tree nodes one level of the list's walk may hold
+constexpr int FR = 64;      // tree nodes one level of the list's walk may hold
 constexpr int MAXSUB = 32;  // sub-patches seeded from the centre
 
 // The features with a lower bound <= reach from c, unranked into tcode / tlb (at most
 // CAP kept; the count returned may exceed it). The tree is walked a level at a time,
 // a lane a node; a level wider than the frontier gives way to every leaf in turn, or,
-// with WIDE_GIVES_UP, ends the walk with a count of LIST_TOO_WIDE (more than any room:
-// the caller reads its points by the tree walk instead).
+// with WIDE_GIVES_UP on a tree of more than WIDE_LEAVES leaves (a scan of them all would
+// cost more than the points' own tree walks), ends the walk with a count of
+// LIST_TOO_WIDE (more than any room: the caller reads its points by the tree walk).
 // *count is a shared counter of the warp; fr two frontier buffers of FR nodes.
 constexpr int LIST_TOO_WIDE = 1 << 28;
+constexpr int WIDE_LEAVES = 4096;
 template <int CAP = MAXC, bool WIDE_GIVES_UP = false>
 __device__ __forceinline__ int warp_list(const DPack& P, const int32_t* leaves, int n_leaves, double3 c, double reach,
                                          uint32_t* tcode, double* tlb, int32_t (*fr)[FR], int* count, int lane) {
@@ -76,7 +78,7 @@ __device__ __forceinline__ int warp_list(const DPack& P, const int32_t* leaves, 
     cur ^= 1;
     ncur = nnext;
   }
-  if (!walked && WIDE_GIVES_UP) {
+  if (!walked && WIDE_GIVES_UP && n_leaves > WIDE_LEAVES) {
     __syncwarp();
     return LIST_TOO_WIDE;
   }

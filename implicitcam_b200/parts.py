@@ -354,6 +354,24 @@ def freeform_patches(seed=0, n=16, size=120.0, base=50.0, bumps=8, degree=3, fac
     return _patched_box(b, degree, degree, knots, knots, net, size, size, cuts, cuts)
 
 
+def ridge_box(fold=0.3, size=30.0, base=13.0, wave=0.0, n=7):
+    """A size x size block whose top is a bicubic B-spline with a knot of full multiplicity
+    at its middle in u: heights base - fold |x - size / 2| (+ wave sin(pi y / size)), so
+    the top folds along x = size / 2 into a ridge, a crease inside the face (the
+    reference's C0 knot line, solid3.rs:1821). n control points a side (odd, 7 or more:
+    the triple knot at 1/2 needs the middle one on the ridge)."""
+    net = np.zeros((n, n, 4))
+    for i in range(n):
+        for j in range(n):
+            x, y = size * i / (n - 1), size * j / (n - 1)
+            net[i, j] = [x, y, base - fold * abs(x - size / 2) + wave * math.sin(math.pi * y / size), 1.0]
+    inner = n - 7
+    ku = [0.0] * 4 + [k / (inner // 2 + 1) * 0.5 for k in range(1, inner // 2 + 1)] + [0.5] * 3 + \
+         [0.5 + k / (inner // 2 + 1) * 0.5 for k in range(1, inner // 2 + 1)] + [1.0] * 4
+    kv = [0.0] * 4 + [k / (n - 3) for k in range(1, n - 3)] + [1.0] * 4
+    return _nurbs_box(SolidBuilder(tol=1e-9), 3, 3, ku, kv, net, size, size)
+
+
 def bump_box():
     """The reference test's bump box (solid3.rs:2092-2147): a 10 x 10 box whose top
     is a biquadratic B-spline over the square, z(5i, 5j) control heights zc."""

@@ -98,10 +98,11 @@ typedef struct IcamBakeStats {
 
 /* Packs the solid for the device (PartGpu::new, partgpu.rs:132; Exact::gpu_pack,
  * crates/icam-core/src/solid3/gpu.rs:259). Returns ICAM_OK and *out, or an error
- * with a message in err. ICAM_ERR_PACK, before any device work, for a B-spline face
- * with a crease along an interior knot line or a side collapsed to a point (a pole):
- * the pack has no knot-line or pole features (Exact::c0_line, solid3.rs:1821-1886;
- * fan_normal, 1960-1986). */
+ * with a message in err. A B-spline face's creases (interior knot lines where its
+ * normal jumps, Exact::c0_line, solid3.rs:1821-1886) are packed as the face's own
+ * edges; ICAM_ERR_PACK, before any device work, for a crease that crosses its face's
+ * loops or a side collapsed to a point (a pole: no pole feature is built, fan_normal,
+ * solid3.rs:1960-1986). */
 int icam_pack_create(const IcamSolidDesc* solid, const IcamPackOptions* opt, IcamPack** out, char* err,
                      size_t errlen);
 

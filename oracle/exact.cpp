@@ -821,7 +821,199 @@ bool Exact::init(const IcamSolidDesc* d, std::string* err) {
   }
   for (auto& e : edges) boxes.push_back(e.box);
   for (auto& v : verts) boxes.push_back({v.p, v.p});
+  // solid3.rs:1609-1614, surface3.rs:1418-1440 c0_lines: a B-spline face's interior knot
+  // lines where its spans' normals differ (sampled at five points a span), each with its
+  // pieces (the after span's side on the line) and the spans either side
+  for (size_t fi = 0; fi < faces.size(); fi++) {
+    const Face& f = faces[fi];
+    if (f.surf.kind != NURBS || !f.surf.ns) continue;
+    const NurbsSurf& ns = *f.surf.ns;
+    auto unit_n = [](const Patch& pa, double s, double t) {
+      SEval e = pa.eval(s, t);
+      return e.ps.cross(e.pt).unit();
+    };
+    for (int k = 0; k < 2; k++) {
+      const int na = k == 0 ? ns.nsu : ns.nsv, nb = k == 0 ? ns.nsv : ns.nsu;
+      for (int a = 1; a < na; a++) {
+        bool crease = false;
+        for (int b = 0; b < nb && !crease; b++) {
+          const Patch& pb = k == 0 ? ns.span(a - 1, b) : ns.span(b, a - 1);
+          const Patch& pn = k == 0 ? ns.span(a, b) : ns.span(b, a);
+          for (double t : {0.0, 0.25, 0.5, 0.75, 1.0}) {
+            V3 n0 = k == 0 ? unit_n(pb, 1.0, t) : unit_n(pb, t, 1.0);
+            V3 n1 = k == 0 ? unit_n(pn, 0.0, t) : unit_n(pn, t, 0.0);
+            if ((n0 - n1).len() > 1e-7) crease = true;
+          }
+        }
+        if (!crease) continue;
+        C0Line l;
+        l.face = int(fi);
+        l.k = k;
+        l.value = k == 0 ? ns.ub[a] : ns.vb[a];
+        for (int b = 0; b < nb; b++) {
+          const Patch& pb = k == 0 ? ns.span(a - 1, b) : ns.span(b, a - 1);
+          const Patch& pn = k == 0 ? ns.span(a, b) : ns.span(b, a);
+          Bez3 z;
+          if (k == 0) {
+            for (int j = 0; j <= pn.dv; j++) z.pw.push_back(pn.at(0, j));
+            z.t0 = pn.v0, z.t1 = pn.v1;
+          } else {
+            for (int i = 0; i <= pn.du; i++) z.pw.push_back(pn.at(i, 0));
+            z.t0 = pn.u0, z.t1 = pn.u1;
+          }
+          l.pieces.push_back(z);
+          l.before.push_back(&pb);
+          l.after.push_back(&pn);
+        }
+        lines.push_back(std::move(l));
+      }
+    }
+  }
+  for (auto& l : lines) {
+    Box b = empty_box();
+    for (auto& z : l.pieces) {
+      Box zb = z.box();
+      grow(b, zb.first);
+      grow(b, zb.second);
+    }
+    boxes.push_back(b);
+  }
   tree_.init(boxes);
+  return true;
+}
+
+// Bernstein coefficients of degree m times those of degree n (degree m + n).
+static std::vector<double> bern_mul(const std::vector<double>& a, const std::vector<double>& b) {
+  const int m = int(a.size()) - 1, n = int(b.size()) - 1;
+  auto binom = [](int N, int K) {
+    double r = 1.0;
+    for (int i = 1; i <= K; i++) r = r * (N - K + i) / i;
+    return r;
+  };
+  std::vector<double> c(m + n + 1, 0.0);
+  for (int i = 0; i <= m; i++)
+    for (int j = 0; j <= n; j++) c[i + j] += binom(m, i) * binom(n, j) / binom(m + n, i + j) * a[i] * b[j];
+  return c;
+}
+static std::vector<double> bern_d(const std::vector<double>& a) {
+  const int m = int(a.size()) - 1;
+  std::vector<double> d(std::max(m, 1), 0.0);
+  for (int i = 0; i < m; i++) d[i] = m * (a[i + 1] - a[i]);
+  return d;
+}
+
+// surface3.rs:734-757 curve_no_critical_point: the rational curve has no point whose
+// chord to p is perpendicular to it (the numerator of d/ds |C - p|^2, in Bernstein form,
+// keeps one sign).
+static bool curve_no_critical_point(const std::vector<H4>& pw, V3 p) {
+  std::vector<double> w, q[3];
+  for (auto& h : pw) {
+    if (!(h[3] > 0.0)) return false;
+    w.push_back(h[3]);
+    q[0].push_back(h[0] - p.x * h[3]);
+    q[1].push_back(h[1] - p.y * h[3]);
+    q[2].push_back(h[2] - p.z * h[3]);
+  }
+  std::vector<double> qu[3] = {bern_d(q[0]), bern_d(q[1]), bern_d(q[2])};
+  auto dot = [](const std::vector<double>* x, const std::vector<double>* y) {
+    std::vector<double> s = bern_mul(x[0], y[0]);
+    for (int k = 1; k < 3; k++) {
+      std::vector<double> t = bern_mul(x[k], y[k]);
+      for (size_t i = 0; i < s.size(); i++) s[i] += t[i];
+    }
+    return s;
+  };
+  std::vector<double> f = bern_mul(w, dot(q, qu)), g = bern_mul(bern_d(w), dot(q, q));
+  for (size_t i = 0; i < f.size(); i++) f[i] -= g[i];
+  auto max_abs = [](const std::vector<double>& x) {
+    double m = 0.0;
+    for (double y : x) m = std::max(m, std::fabs(y));
+    return m;
+  };
+  double q0 = std::max(max_abs(q[0]), std::max(max_abs(q[1]), max_abs(q[2])));
+  double q1 = std::max(max_abs(qu[0]), std::max(max_abs(qu[1]), max_abs(qu[2])));
+  double size = max_abs(w) * 3.0 * q0 * q1 + max_abs(bern_d(w)) * 3.0 * q0 * q0;
+  double lo = INF, hi = -INF;
+  for (double x : f) lo = std::min(lo, x), hi = std::max(hi, x);
+  return lo > 1e-11 * size || hi < -1e-11 * size;
+}
+
+// solid3.rs:1821-1886 c0_line: the nearest point of a knot line inside its face below
+// `cutoff` where the distance along the line is critical (where the line meets the face's
+// boundary the edges answer): its distance, the point, and the two sides' outward normals
+// summed (the span before the line at its far side, the span after at its near side).
+bool Exact::c0_line(const C0Line& l, V3 p, double cutoff, ExactStats* st, double* d_out, V3* q_out,
+                    V3* n_out) const {
+  const Face& f = faces[l.face];
+  auto at = [&](double w) { return l.k == 0 ? P2{l.value, w} : P2{w, l.value}; };
+  struct E {
+    double lb;
+    size_t i;
+    Bez3 z;
+    int depth;
+  };
+  std::vector<E> heap;
+  for (size_t i = 0; i < l.pieces.size(); i++) {
+    double lb = box_dist(p, l.pieces[i].box());
+    if (lb < cutoff) heap.push_back({lb, i, l.pieces[i], 0});
+  }
+  double bound = cutoff;
+  bool have = false;
+  double bd = 0.0, bw = 0.0;
+  V3 bq;
+  size_t bi = 0;
+  int pops = 0;
+  while (!heap.empty()) {
+    size_t k = 0;
+    for (size_t j = 1; j < heap.size(); j++)
+      if (heap[j].lb < heap[k].lb) k = j;
+    E e = heap[k];
+    heap[k] = heap.back();
+    heap.pop_back();
+    if (e.lb >= bound - DIST_EPS) break;
+    if (++pops > 4096) {
+      st->capped = true;
+      break;
+    }
+    P2 a = at(e.z.t0), b = at(e.z.t1);
+    int state = f.trim.box_class({std::min(a[0], b[0]), std::min(a[1], b[1])}, {std::max(a[0], b[0]), std::max(a[1], b[1])});
+    if (state == 0) continue;
+    double s = e.z.newton(p, 0.5);
+    Eval3 ev = e.z.eval(s);
+    double d = (ev.p - p).len();
+    double w = e.z.t0 + s * (e.z.t1 - e.z.t0);
+    P2 uv = at(w);
+    if (d < bound && (state == 1 || f.trim.inside(uv[0], uv[1]))) {
+      bound = d;
+      V3 r = ev.p - p;
+      auto big = [](V3 x) { return std::max(std::fabs(x.x), std::max(std::fabs(x.y), std::fabs(x.z))); };
+      double round = 1024.0 * 2.220446049250313e-16 * (big(ev.p) + big(p) + d);
+      if (std::fabs(r.dot(ev.d1)) <= (round + 1e-12 * ev.d1.len()) * ev.d1.len()) {
+        have = true;
+        bd = d, bq = ev.p, bi = e.i, bw = w;
+      }
+    }
+    if (e.depth >= 40 || curve_no_critical_point(e.z.pw, p)) continue;
+    auto lr = e.z.split(0.5);
+    for (const Bez3* c : {&lr.first, &lr.second}) {
+      double lbc = box_dist(p, c->box());
+      if (lbc < bound - DIST_EPS) heap.push_back({lbc, e.i, *c, e.depth + 1});
+    }
+  }
+  st->pops += pops;
+  if (!have) return false;
+  auto side_n = [&](const Patch* pa, double side) {
+    double s, t;
+    if (l.k == 0)
+      s = side, t = (bw - pa->v0) / (pa->v1 - pa->v0);
+    else
+      s = (bw - pa->u0) / (pa->u1 - pa->u0), t = side;
+    SEval e = pa->eval(s, t);
+    return e.ps.cross(e.pt).unit();
+  };
+  *n_out = (side_n(l.before[bi], 1.0) + side_n(l.after[bi], 0.0)) * f.sense;
+  *d_out = bd;
+  *q_out = bq;
   return true;
 }
 
@@ -898,11 +1090,16 @@ Sd Exact::sdf_within(V3 p, double bound, ExactStats* st) const {
         best = {c.dist * sign((p - c.q).dot(pn)), c.q, 1, int(ei), false};
         cusp = pn.len() < 1e-9;
       }
-    } else {
+    } else if (id < nF + nE + verts.size()) {
       size_t vi = id - nF - nE;
       const Vert& v = verts[vi];
       double d = (p - v.p).len();
       if (d < cur) best = {d * sign((p - v.p).dot(v.pn)), v.p, 2, int(vi), false};
+    } else {  // solid3.rs:1790-1795 a knot line
+      const C0Line& l = lines[id - nF - nE - verts.size()];
+      double d;
+      V3 q, n;
+      if (c0_line(l, p, cur, st, &d, &q, &n)) best = {d * sign((p - q).dot(n)), q, 0, l.face, false};
     }
     if (best.d != before) {
       found = true;
@@ -929,8 +1126,10 @@ std::vector<size_t> Exact::candidates(V3 c, double r, double d) const {
     } else if (id < nF + nE) {
       const Edge3& e = edges[id - nF].curve;
       lb = e.kind <= 1 ? e.closest(c).dist : 0.0;
-    } else {
+    } else if (id < nF + nE + verts.size()) {
       lb = (c - verts[id - nF - nE].p).len();
+    } else {
+      lb = box_dist(c, tree_.boxes_of(id));
     }
     if (lb <= reach) out.push_back(id);
   });
@@ -942,7 +1141,8 @@ std::vector<size_t> Exact::candidates(V3 c, double r, double d) const {
 int Exact::kind_of(size_t id) const {
   if (id < nf()) return faces[id].surf.kind == NURBS ? 1 : 0;
   if (id < nf() + ne()) return edges[id - nf()].curve.kind <= 1 ? 2 : 3;
-  return 4;
+  if (id < nf() + ne() + nv()) return 4;
+  return 3;  // a knot line: as a spline edge
 }
 
 // partcache.rs:962-970 packed

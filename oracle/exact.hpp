@@ -163,6 +163,21 @@ class BoxTree {
   }
 };
 
+// solid3.rs:1562-1568 C0Line: an interior knot line of a B-spline face where the surface
+// is only C0 (a crease): the direction held fixed (0: u), its value, and per span of the
+// other direction the line's piece (parameter along the line) with the spans before and
+// after it. Found here from the surface's geometry (the spans' normals differ across the
+// line), where the reference takes the knots of full multiplicity: a knot line across
+// which the normal is continuous needs no line of its own (its nearest points are
+// critical points of the spans on either side).
+struct C0Line {
+  int face = 0;
+  int k = 0;
+  double value = 0;
+  std::vector<Bez3> pieces;
+  std::vector<const Patch*> before, after;
+};
+
 class Exact {
  public:
   bool init(const IcamSolidDesc* d, std::string* err);
@@ -179,9 +194,11 @@ class Exact {
   std::vector<Face> faces;
   std::vector<EdgeRec> edges;
   std::vector<Vert> verts;
+  std::vector<C0Line> lines;  // the tree's ids after the vertices
   Box bbox;
 
  private:
+  bool c0_line(const C0Line& l, V3 p, double cutoff, ExactStats* st, double* d, V3* q, V3* n) const;
   BoxTree tree_;
   bool face(size_t fi, V3 p, double cutoff, ExactStats* st, double* d, V3* q, V3* n) const;
   V3 normal_at(size_t fi, V3 x) const;
