@@ -131,6 +131,14 @@ def workload_name(kind):
     return f"freeform-top level bake, h={H} mm, band +-{BAND} mm"
 
 
+def level_config(args, nb):
+    """The level both arms (the GPU bake and the CPU reference) measure: the same dict in
+    both lines. precision names the GPU line's headline arm; the CPU arm is f64 (its dtype)."""
+    return {"workload": workload_name(args.workload), "part": "mold" if args.workload == "mold" else "freeform_top",
+            "seed": "rank", "h_mm": H, "band_mm": BAND, "nb": [int(x) for x in nb], "precision": args.precision,
+            "l2": "flushed (256 MB write) before every step"}
+
+
 def sample_clocks(path):
     q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -238,7 +246,7 @@ def run_reference(args, rank, world):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "voxels/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": workload_name(args.workload), "seed": 0},
+        "config": level_config(args, workload(0, kind=args.workload)[2]),
         "cpu_baseline": {"value": value, "unit": "voxels/s", "cores": cores, "kind": "port",
                          "sample": f"each step: {sample}"},
         "e2e": {"value": value, "unit": "voxels/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -402,10 +410,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == part_gpu.FP64 else "f32+f64",
             "data": "synthetic",
-            "config": {"workload": workload_name(args.workload),
-                       "part": "mold" if args.workload == "mold" else "freeform_top",
-                       "seed": "rank", "h_mm": H, "band_mm": BAND, "nb": nb.tolist(), "precision": args.precision,
-                       "l2": "flushed (256 MB write) before every step"},
+            "config": level_config(args, nb),
             "speedup_vs_fp64": value / others["fp64"]["value"] if "fp64" in others else None,
             "fp64": others.get("fp64"), "mixed": others.get("mixed"), "error_vs_oracle": error, "seednet": seednet,
             "bricks_read": st["bricks_read"], "bricks_stored": st["bricks_words"],

@@ -119,6 +119,12 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 2) k_bricks_t(BrickArgs a) {
     }
     // ---- 1. list
     int n = warp_list(P, leaves, n_leaves, c, reach, S.u.list.code, S.u.list.lb, S.u.list.fr, &S.n, lane);
+    // a list past its room taken again with a shorter reach (bricks_mixed.cu, step 1)
+    double reach_ok = INFINITY;
+    for (int tries = 0; n > MAXC && tries < 4; tries++) {
+      reach_ok = (tries == 0 ? reach : reach_ok) * 0.8;
+      n = warp_list(P, leaves, n_leaves, c, reach_ok, S.u.list.code, S.u.list.lb, S.u.list.fr, &S.n, lane);
+    }
     const bool overflow = n > MAXC;
     if (overflow) n = MAXC;
     warp_rank(S.u.list.code, S.u.list.lb, n, S.code, S.lb, lane);
@@ -171,7 +177,7 @@ __global__ void __launch_bounds__(MAX_WARPS * 32, 2) k_bricks_t(BrickArgs a) {
     // ---- 3. every node: the warp's lanes walk the same ranked candidates together
     int cnt[3] = {0, 0, 0};
     int pending = 0;
-    const WarpCands W{S.code, S.lb, nullptr, S.cert, S.slot, S.v.seed, S.net, S.net32, n, overflow};
+    const WarpCands W{S.code, S.lb, nullptr, S.cert, S.slot, S.v.seed, S.net, S.net32, n, overflow, reach_ok};
     for (int nn0 = 0; nn0 < 729; nn0 += 32) {
       const int nn = nn0 + lane;
       const bool live = nn < 729;

@@ -54,8 +54,6 @@ struct BrickSmemF {
   int n;
 };
 static_assert(sizeof(((BrickSmemF*)0)->x) >= SN_ROOM, "the seed network's room");
-static_assert(sizeof(BrickSmemF) % 16 == 0 && SN_WBYTES % 16 == 0, "the staged weights are 16-byte aligned");
-static_assert(2 * (sizeof(BrickSmemF) * MW + SN_WBYTES) <= 227 * 1024, "two blocks a SM with the weights staged");
 
 // The i16 step's half: a distance below it (less the float error) rounds to zero on
 // either side of the surface, so a bake that keeps only i16 values needs no sign for it.
@@ -84,16 +82,6 @@ __global__ void __launch_bounds__(MW * 32, ICAM_MIXED_BLOCKS) k_bricks_m(BrickAr
   const int warps = int(blockDim.x >> 5);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   BrickSmemF& S = smem[warp];
-  // the seed network's weights, staged once a block behind the warps' rooms (one part
-  // a launch: a batch's parts each have their own, read from global memory)
-  const void* net_staged = nullptr;
-  if (!BATCH && a.net_w) {
-    uint4* dst = reinterpret_cast<uint4*>(smem_raw + sizeof(BrickSmemF) * warps);
-    const uint4* src = static_cast<const uint4*>(a.net_w);
-    for (int i = threadIdx.x; i < int(SN_WBYTES / 16); i += blockDim.x) dst[i] = src[i];
-    __syncthreads();
-    net_staged = dst;
-  }
   unsigned long long* work = a.stats ? a.stats + 15 : nullptr;
   if (lane == 0) mbar_init(&S.bar);
   __syncwarp();
@@ -113,7 +101,10 @@ __global__ void __launch_bounds__(MW * 32, ICAM_MIXED_BLOCKS) k_bricks_m(BrickAr
     const int32_t* leaves = BATCH ? Q->leaves : a.leaves;
     const int32_t n_leaves = BATCH ? Q->n_leaves : a.n_leaves;
     const float* net_feat = BATCH ? Q->net_feat : a.net_feat;
-    const void* net_w = BATCH ? Q->net_w : net_staged;
+    // the seed network's weights are read through L1 from global memory: staged in shared
+    // memory they took 25 KB a block of the L1 the kernel's spills live in (measured:
+    // learned node phase 28.7 ms staged, 27.4 ms read)
+    const void* net_w = BATCH ? Q->net_w : a.net_w;
     const double3 first = mk(a.firsts[3 * bi], a.firsts[3 * bi + 1], a.firsts[3 * bi + 2]);
     const double half = 4.0 * h;
     const double3 c = first + mk(half, half, half);
@@ -148,6 +139,14 @@ __global__ void __launch_bounds__(MW * 32, ICAM_MIXED_BLOCKS) k_bricks_m(BrickAr
     }
     // ---- 1. list
     int n = warp_list(P, leaves, n_leaves, c, reach, S.x.w.u.list.code, S.x.w.u.list.lb, S.x.w.u.list.fr, &S.n, lane);
+    // a list past its room is taken again with a shorter reach (down to 0.8^4 of it) until
+    // it fits: its nodes whose answer lies within the shorter reach (less their distance
+    // from the centre) need nothing more, the rest go to the tree walk
+    double reach_ok = INFINITY;
+    for (int tries = 0; n > MAXC && tries < 4; tries++) {
+      reach_ok = (tries == 0 ? reach : reach_ok) * 0.8;
+      n = warp_list(P, leaves, n_leaves, c, reach_ok, S.x.w.u.list.code, S.x.w.u.list.lb, S.x.w.u.list.fr, &S.n, lane);
+    }
     const bool overflow = n > MAXC;
     if (overflow) n = MAXC;
     warp_rank(S.x.w.u.list.code, S.x.w.u.list.lb, n, S.code, S.lb64, lane);
@@ -301,7 +300,8 @@ __global__ void __launch_bounds__(MW * 32, ICAM_MIXED_BLOCKS) k_bricks_m(BrickAr
     int cnt[3] = {0, 0, 0};
     int pending = 0, n_evals = 0, n_solves = 0;
     {
-      const WarpCandsF W{S.code, S.lbf, S.lbs, S.cert, S.slot, S.v.seed, S.geo, S.net32, S.x.w.res, S.rslot, n, 8};
+      const WarpCandsF W{S.code, S.lbf, S.lbs, S.cert, S.slot, S.v.seed, S.geo, S.net32, S.x.w.res, S.rslot, n, 8,
+                         float(reach_ok * (1.0 - 1e-6)) - 1e-5f};
       int lastk = -1;
       float ls = 0.f, lt = 0.f;
       const float hf = float(h);
@@ -343,7 +343,8 @@ __global__ void __launch_bounds__(MW * 32, ICAM_MIXED_BLOCKS) k_bricks_m(BrickAr
       }
       __syncwarp();
       // the double walk's list: the same candidates, centre starts (no seeds)
-      const WarpCands W64{S.code, S.lb64, net_w ? S.lbs : nullptr, S.cert, nullptr, nullptr, S.net, S.net32, n, overflow};
+      const WarpCands W64{S.code, S.lb64, net_w ? S.lbs : nullptr, S.cert, nullptr, nullptr, S.net, S.net32, n, overflow,
+                          reach_ok};
       int tail = 0;
       for (int b0 = 0; b0 < npend; b0 += 32) {
         const bool live = b0 + lane < npend;
@@ -410,9 +411,9 @@ void launch_bricks_mixed(const BrickArgs& a, cudaStream_t s, int warps) {
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const bool batch = a.parts != nullptr;
-  const size_t smem = sizeof(BrickSmemF) * warps + (!batch && a.net_w ? SN_WBYTES : 0);
+  const size_t smem = sizeof(BrickSmemF) * warps;
   auto kern = batch ? k_bricks_m<true> : k_bricks_m<false>;
-  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(BrickSmemF) * MW + SN_WBYTES));
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(BrickSmemF) * MW));
   int per_sm = 1;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, warps * 32, smem);
   const int64_t want = (a.n + warps - 1) / warps;

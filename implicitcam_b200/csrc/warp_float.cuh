@@ -151,6 +151,9 @@ struct WarpCandsF {
   const int8_t* rslot;
   int n;
   int iters;           // float Newton iterations a solve
+  // every feature whose bound from the centre is at most this is in the list (a list
+  // taken again with a shorter reach; infinite when whole), less the float error
+  float reach_ok = INFINITY;
 };
 
 // The float walk of the lane's node (pc: its offset from the centre; p: the node in
@@ -261,6 +264,7 @@ __device__ __forceinline__ int warp_point_f(const DPack& P, const WarpCandsF& W,
     }
   }
   if (!live) return 1;
+  if (best > W.reach_ok - rr) pend = true;  // a feature the shortened list left out may be nearer
   if (wk >= 0) *lastk = wk, *ls = ws, *lt = wt;
   if (!pend && nd > 0 && und < best) {  // the deferred sub-patches, by the double subdivision
     if (nd > 2) {

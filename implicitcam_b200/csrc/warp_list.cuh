@@ -239,6 +239,11 @@ struct WarpCands {
   float4* net32;
   int n;
   bool overflow;  // more candidates than the list holds: every point walks the tree
+  // The list holds every feature whose bound from the centre is at most this (a list
+  // taken again with a shorter reach when the whole one overflowed; infinite when whole):
+  // a point whose answer is farther than reach_ok less its distance from the centre is
+  // handed back for the tree walk.
+  double reach_ok = INFINITY;
 };
 
 // The value of point p (lane's own; `live` false for a lane without one) over the ranked
@@ -360,12 +365,12 @@ __device__ __forceinline__ void warp_point(const DPack& P, const WarpCands& W, d
   if (!live) return;
   // !TAIL: a point the list leaves undecided is handed back (flag 3) for the caller to
   // read by the whole tree walk later, out of the loop that calls this one
-  if (!TAIL && (W.overflow || (und < best && und <= cap))) {
+  if (!TAIL && (W.overflow || (und < best && und <= cap) || best > W.reach_ok - rr)) {
     *value = NAN, *flag = 3;
     return;
   }
   if (nd > 0 && nd <= 2 && und < best && und <= cap) point_resolve(P, p, dc0, dl0, dc1, dl1, nd, &best, &sdv, &und);
-  if (W.overflow || (und < best && und <= cap)) {
+  if (W.overflow || (und < best && und <= cap) || best > W.reach_ok - rr) {
     point_fallback(P, p, cap, value, flag);
   } else if (!isnan(sdv) && best <= cap) {
     *value = sdv, *flag = 0;
