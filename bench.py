@@ -43,10 +43,11 @@ BAND = 2.0
 # B-spline span, line or arc edge, spline edge piece, vertex): foot + uv + one parity
 # leg; 6 Newton steps of 750 + trim 200; closed-form foot; 6 steps of 120; a distance
 FLOPS_PER_CANDIDATE = np.array([80.0, 6 * 750.0 + 200.0, 40.0, 6 * 120.0, 10.0])
-# DRAM bytes k_bricks moves a read brick: one ncu capture of the same kernel (mixed form)
-# on the same part's level at h = 0.2 mm, 7x smaller (8.55 GB/s x 13.06 ms = 111.7 MB
-# over 129,053 read bricks), scaled by the bricks read
-TRAFFIC_PER_READ_BRICK = 8.551313e9 * 13.0616e-3 / 129053
+# DRAM bytes the brick kernel moves a read brick: one ncu capture of the same kernel
+# (mixed form) on the same part's level at h = 0.2 mm, 7x smaller (dram__bytes_read.sum
+# 12.51 MB + dram__bytes_write.sum 102.30 MB over 129,053 read bricks), scaled by the
+# bricks read
+TRAFFIC_PER_READ_BRICK = (12.513024e6 + 102.296832e6) / 129053
 # the seed network's training: 50M pairs from the exact evaluator, before any timing
 SEEDNET_STEPS, SEEDNET_BATCH = 12208, 4096
 
