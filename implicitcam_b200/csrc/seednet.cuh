@@ -69,7 +69,9 @@ __device__ __forceinline__ void sn_layer(__nv_bfloat16* act, const __nv_bfloat16
 #pragma unroll
     for (int mt = 0; mt < 2; mt++) acc[mt][nt][0] = b0, acc[mt][nt][1] = b1, acc[mt][nt][2] = b0, acc[mt][nt][3] = b1;
   }
-#pragma unroll
+  // the k-steps one at a time (not unrolled): a quarter of the code beside the brick
+  // kernel's walk in the instruction cache (measured: learned node phase 27.2 -> 26.9 ms)
+#pragma unroll 1
   for (int ks = 0; ks < K / 16; ks++) {
     uint32_t a[2][4];
 #pragma unroll
