@@ -308,6 +308,11 @@ def main():
     g = part_gpu.PartGpu(b, need=need, device=local)
     stream = torch.cuda.ExternalStream(g.stream(), device=local)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")  # > L2 (126 MB)
+    # the level's narrow band as the reference's decision defines it (the bricks its box
+    # rule reads, partcache.rs:226-331): the voxel count of every arm and of the CPU
+    # reference, read once before any timing; a bake's tighter rule reads fewer of them
+    # (bricks_read_bake) with the same map and atlas
+    band_bricks = int(g.decide(H, lo, nb, BAND, precision=part_gpu.FP64)[3]["bricks_read"])
     seednet = None
     if prec == part_gpu.MIXED_LEARNED:  # trained before any timing: 50M pairs from the exact evaluator
         t0 = time.perf_counter()
@@ -344,7 +349,7 @@ def main():
             ms.append(t)
             stats.append(st)
         torch.cuda.synchronize()
-        total_ms, voxels = over_ranks(dist, f"cuda:{local}", float(sum(ms)), 512.0 * stats[-1]["bricks_read"])
+        total_ms, voxels = over_ranks(dist, f"cuda:{local}", float(sum(ms)), 512.0 * band_bricks)
         if dist:
             dist.barrier()
         return total_ms, voxels, stats
@@ -414,7 +419,7 @@ def main():
             "config": level_config(args, nb),
             "speedup_vs_fp64": value / others["fp64"]["value"] if "fp64" in others else None,
             "fp64": others.get("fp64"), "mixed": others.get("mixed"), "error_vs_oracle": error, "seednet": seednet,
-            "bricks_read": st["bricks_read"], "bricks_stored": st["bricks_words"],
+            "bricks_read": band_bricks, "bricks_read_bake": st["bricks_read"], "bricks_stored": st["bricks_words"],
             "bricks_settled": st["bricks_settled"],
             "nodes_exact": st["nodes_exact"], "nodes_undecided": st["nodes_undecided"],
             **newton_figures(st),
@@ -590,6 +595,8 @@ def run_batch(args, rank, world):
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
     batch = part_gpu.Batch(gs)
+    # the parts' narrow bands as the reference's decision defines them (their voxel count)
+    band_bricks = sum(int(g.decide(*L, precision=part_gpu.FP64)[3]["bricks_read"]) for g, L in zip(gs, levels))
 
     def timed(p):
         for _ in range(args.warmup):
@@ -603,7 +610,7 @@ def run_batch(args, rank, world):
     arms = {}
     for name, p in precs.items():
         t, st = timed(p)
-        arms[name] = {"ms_per_step": 1e3 * t, "value": 512.0 * st["bricks_read"] / t,
+        arms[name] = {"ms_per_step": 1e3 * t, "value": 512.0 * band_bricks / t,
                       "ms_decide": st["ms_decide"], "ms_bricks": st["ms_bricks"], "warps": st["warps"],
                       "graph_replayed": st["graph_replayed"]}
     t_batch, st = timed(prec)
@@ -618,7 +625,7 @@ def run_batch(args, rank, world):
             if len(per_part) < len(gs):
                 per_part.append(s1["bricks_read"])
     t_alone = (time.perf_counter() - t0) / args.steps
-    voxels = 512.0 * st["bricks_read"]
+    voxels = 512.0 * band_bricks
     error = None
     if rank == 0 and not args.no_cpu:
         # the checker, outside every timed region: one part of each family

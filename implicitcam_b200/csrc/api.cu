@@ -360,6 +360,7 @@ int decide_level(IcamPack* pk, const LevelDesc& L, DecideOut* out) {
     a.n_read = cnt + 1;
     const bool is_first = launches == 0;
     a.n_double = cnt + 2;
+    a.tight = L.tight ? 1 : 0;
     if (is_first) {
       a.first_sd = static_cast<double*>(d_first);
       a.first_sign = reinterpret_cast<int8_t*>(static_cast<double*>(d_first) + ncur);
@@ -427,6 +428,7 @@ static int bake_level(IcamPack* pk, double h, const double lo[3], const int64_t 
   for (int k = 0; k < 3; k++) L.lo[k] = lo[k], L.nb[k] = nb[k], L.origin[k] = origin ? origin[k] : 0.0;
   L.has_origin = origin != nullptr;
   L.precision = precision;
+  L.tight = true;  // a bake: the map and words of the reference's rule with fewer reads
   cudaEvent_t ev[5];
   for (auto& e : ev) CK(cudaEventCreate(&e));
   CK(cudaEventRecord(ev[0], s));

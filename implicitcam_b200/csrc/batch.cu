@@ -261,6 +261,7 @@ int icam_batch_bake(IcamBatch* bt, const IcamBatchLevel* levels, int precision, 
     a.size = size;
     a.h = lv.h;
     a.clamp = lv.clamp;
+    a.tight = 1;  // a bake: the decision's tight rule (same maps and words, fewer reads)
     for (int k = 0; k < 3; k++) a.lo[k] = lv.lo[k], a.nb[k] = lv.nb[k];
     a.next_cap = box_off[i + 1] - box_off[i];
     a.read_cap = total;

@@ -36,6 +36,15 @@ struct DecideSmem {
 };
 static_assert(sizeof(DecideSmem) * DWARPS <= 48 * 1024, "static shared memory of a block");
 
+// A box's radius from its corners grown by the clamp (lo, hi): the reference's, half
+// their diagonal; under the tight rule (a level bake), the box's own half-diagonal,
+// rounded up.
+__device__ __forceinline__ double box_radius(const DecideArgs& a, double3 lo, double3 hi) {
+  if (!a.tight) return 0.5 * len(hi - lo);
+  const double g = 2.0 * a.clamp;
+  return 0.5 * len(hi - lo - mk(g, g, g)) * (1.0 + 1e-12);
+}
+
 // One box's verdict from its centre's value (v, f) read within `cut` (partcache.rs:370-383:
 // decided once the centre is known past the box grown by the clamp), the map entries it
 // settles, and its children (up to 8: into kids, *nk of them, for the caller to append;
@@ -108,7 +117,7 @@ __device__ void decide_box(const DecideArgs& a, long long size, const Box4& b, d
       k.reach = len((klo + khi) * 0.5 - c);
       k.parent_sd = sd;
       if (by_bound) {
-        const double rk = 0.5 * len(khi - klo);
+        const double rk = box_radius(a, klo, khi);
         const double bound = fabs(sd) - verr - k.reach;
         const double dcb = copysign(bound, sd);
         if (fabs(sd) + verr + k.reach < (rk + a.clamp) * (1.0 - 1e-12) && bound > 0.0 &&
@@ -174,7 +183,7 @@ __device__ __forceinline__ void decide_group(const DecideArgs& a, const Box4* bo
   double3 hi = mk(a.lo[0] + side * (b.x + size) + a.clamp, a.lo[1] + side * (b.y + size) + a.clamp,
                   a.lo[2] + side * (b.z + size) + a.clamp);
   const double3 c = (lo + hi) * 0.5;
-  const double r = 0.5 * len(hi - lo);
+  const double r = box_radius(a, lo, hi);
   const double cut = (r + a.clamp) * (1.0 + 1e-4);
   const int glanes = int(min(int64_t(gs), n - g0));  // lanes of the group holding a box
   double v = 0.0;
@@ -290,7 +299,7 @@ __device__ __forceinline__ void decide_group_f(const DecideArgs& a, const Box4* 
   double3 hi = mk(a.lo[0] + side * (b.x + size) + a.clamp, a.lo[1] + side * (b.y + size) + a.clamp,
                   a.lo[2] + side * (b.z + size) + a.clamp);
   const double3 c = (lo + hi) * 0.5;
-  const double r = 0.5 * len(hi - lo);
+  const double r = box_radius(a, lo, hi);
   const double cut = (r + a.clamp) * (1.0 + 1e-4);
   const int glanes = int(min(int64_t(gs), n - g0));  // lanes of the group holding a box
   double v = 0.0, verr = 0.0;
@@ -446,7 +455,7 @@ __device__ __forceinline__ void box_geometry(const DecideArgs& a, const Box4& b,
   double3 hi = mk(a.lo[0] + side * (b.x + size) + a.clamp, a.lo[1] + side * (b.y + size) + a.clamp,
                   a.lo[2] + side * (b.z + size) + a.clamp);
   *c = (lo + hi) * 0.5;
-  *r = 0.5 * len(hi - lo);
+  *r = box_radius(a, lo, hi);
   *cut = (*r + a.clamp) * (1.0 + 1e-4);
 }
 

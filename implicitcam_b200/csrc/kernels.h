@@ -88,6 +88,12 @@ struct DecideArgs {
   long long first_dims[3];
   // the mixed form: centres the float walk left to the double walk (counted; or null)
   unsigned long long* n_double;
+  // 0: the reference's rule (a box's radius is that of the box grown by the clamp,
+  // partcache.rs:341-423); 1: a level bake's, the box's own radius: a box whose centre
+  // lies farther than that plus the clamp from the surface has every node past the
+  // clamp, so each of its bricks would be read into air or material. The map and words
+  // are the same; fewer boxes and bricks are read, with shorter cuts.
+  int32_t tight;
 };
 
 __global__ void k_points(DPack P, const double* xyz, int64_t n, double cap, double* value, int8_t* flag);

@@ -37,6 +37,7 @@ struct LevelDesc {
   int64_t nb[3] = {0, 0, 0};
   bool has_origin = false;
   int precision = 0;  // ICAM_FP64, ICAM_MIXED or ICAM_MIXED_LEARNED
+  bool tight = false;  // the decision's tight rule (DecideArgs::tight): a level bake's
 };
 
 // The box decision of a level, left on the device in the pack's scratch: the map (read

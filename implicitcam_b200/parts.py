@@ -360,6 +360,8 @@ def ridge_box(fold=0.3, size=30.0, base=13.0, wave=0.0, n=7):
     the top folds along x = size / 2 into a ridge, a crease inside the face (the
     reference's C0 knot line, solid3.rs:1821). n control points a side (odd, 7 or more:
     the triple knot at 1/2 needs the middle one on the ridge)."""
+    if n < 7 or n % 2 == 0:
+        raise ValueError("ridge_box needs an odd n of 7 or more")
     net = np.zeros((n, n, 4))
     for i in range(n):
         for j in range(n):

@@ -107,8 +107,13 @@ int oracle_candidates(void* h, const double* c, double r, double d, int32_t* out
 // corner. Returns the number of bricks to read (written to read_idx / read_d up to
 // cap), and the map (nb[0]*nb[1]*nb[2] entries) with AIR/SOLID decided and
 // ORACLE_READ at bricks to read.
-int64_t oracle_decide(void* h, double hcell, const double* lo3, const int64_t* nb, double clamp, const double* origin,
-                      int threads, uint32_t* map, int64_t* read_idx, double* read_d, int64_t cap) {
+// With tight != 0 a box's radius is the half diagonal of its own nodes' box instead of
+// the box grown by the clamp: every node still lies within it of the centre, so a box
+// it decides AIR (SOLID) holds only nodes past the clamp, which the reference's rule
+// reads and packs as an AIR (SOLID) brick. The map after the bricks are read is the same.
+int64_t oracle_decide_rule(void* h, double hcell, const double* lo3, const int64_t* nb, double clamp,
+                           const double* origin, int threads, int tight, uint32_t* map, int64_t* read_idx,
+                           double* read_d, int64_t cap) {
   auto* ex = static_cast<Exact*>(h);
   V3 lo(lo3[0], lo3[1], lo3[2]);
   double side = 8.0 * hcell;
@@ -141,7 +146,7 @@ int64_t oracle_decide(void* h, double hcell, const double* lo3, const int64_t* n
       int64_t b2[3] = {a[0] + size, a[1] + size, a[2] + size};
       V3 p = first(a) - V3(clamp, clamp, clamp), q = first(b2) + V3(clamp, clamp, clamp);
       V3 c((p.x + q.x) * 0.5, (p.y + q.y) * 0.5, (p.z + q.z) * 0.5);
-      double r = 0.5 * (q - p).len();
+      double r = tight ? 0.5 * (first(b2) - first(a)).len() : 0.5 * (q - p).len();
       ExactStats st;
       Sd s = ex->sdf(c, &st);
       if (s.unsure) {
@@ -186,6 +191,11 @@ int64_t oracle_decide(void* h, double hcell, const double* lo3, const int64_t* n
     size /= 2;
   }
   return nread;
+}
+
+int64_t oracle_decide(void* h, double hcell, const double* lo3, const int64_t* nb, double clamp, const double* origin,
+                      int threads, uint32_t* map, int64_t* read_idx, double* read_d, int64_t cap) {
+  return oracle_decide_rule(h, hcell, lo3, nb, clamp, origin, threads, 0, map, read_idx, read_d, cap);
 }
 
 // partcache.rs:979-1058 exact_brick: the 729 nodes of each brick whose first node is

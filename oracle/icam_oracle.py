@@ -45,6 +45,9 @@ def lib():
         L.oracle_decide.restype = C.c_int64
         L.oracle_decide.argtypes = [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_int,
                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64]
+        L.oracle_decide_rule.restype = C.c_int64
+        L.oracle_decide_rule.argtypes = [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p,
+                                         C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64]
         L.oracle_bricks.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_double, C.c_double, C.c_int,
                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         _lib = L
@@ -99,8 +102,11 @@ class Oracle:
         n = lib().oracle_candidates(self.h, _p(c), float(r), float(d), _p(out), 4096, _p(kinds))
         return out[:n].copy(), kinds[:n].copy()
 
-    def decide(self, h, lo, nb, clamp, origin=None, threads=None):
-        """The level's brick map and the bricks to read (partcache.rs:226-331)."""
+    def decide(self, h, lo, nb, clamp, origin=None, threads=None, tight=False):
+        """The level's brick map and the bricks to read (partcache.rs:226-331).
+
+        tight=True bounds each box by its own nodes' half diagonal rather than that of
+        the box grown by the clamp (the rule the library's bakes use)."""
         lo = np.ascontiguousarray(lo, dtype=np.float64)
         nb = np.ascontiguousarray(nb, dtype=np.int64)
         origin = lo + h if origin is None else np.ascontiguousarray(origin, dtype=np.float64)
@@ -109,8 +115,8 @@ class Oracle:
         cap = total
         idx = np.zeros(cap, np.int64)
         dc = np.zeros(cap)
-        n = lib().oracle_decide(self.h, float(h), _p(lo), _p(nb), float(clamp), _p(origin), threads or self.threads,
-                                _p(m), _p(idx), _p(dc), cap)
+        n = lib().oracle_decide_rule(self.h, float(h), _p(lo), _p(nb), float(clamp), _p(origin),
+                                     threads or self.threads, int(bool(tight)), _p(m), _p(idx), _p(dc), cap)
         return m, idx[:n].copy(), dc[:n].copy()
 
     def bricks(self, firsts, h, clamp, threads=None):

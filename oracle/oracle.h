@@ -25,6 +25,9 @@ void oracle_sdf(void* h, const double* pts, int64_t n, double bound, double* d_o
 int oracle_candidates(void* h, const double* c, double r, double d, int32_t* out, int cap, int32_t* kinds);
 int64_t oracle_decide(void* h, double hcell, const double* lo, const int64_t* nb, double clamp, const double* origin,
                       int threads, uint32_t* map, int64_t* read_idx, double* read_d, int64_t cap);
+int64_t oracle_decide_rule(void* h, double hcell, const double* lo, const int64_t* nb, double clamp,
+                           const double* origin, int threads, int tight, uint32_t* map, int64_t* read_idx,
+                           double* read_d, int64_t cap);
 void oracle_bricks(void* h, const double* firsts, int64_t n, double hcell, double clamp, int threads, double* f_out,
                    int16_t* q_out, int32_t* kind_out, uint32_t* words_out);
 
