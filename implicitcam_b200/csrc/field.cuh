@@ -195,8 +195,12 @@ HDI void bb_sub(const DPack& P, int si, double3 p, Acc& A) {
       }
     }
     if (cert && conv) continue;  // its one minimum is known
-    {
-      // no critical point in the part: nothing of the face's is here (surface3.rs:1280-1282)
+    // no critical point in the part: nothing of the face's is here (surface3.rs:1280-1282);
+    // a part touching a pole's side is never cleared (the distance's minimum at the pole
+    // need not be a critical point of the part's parameters)
+    const bool pole = ((s.pole_sides & 1) && r.s0 == 0.0) || ((s.pole_sides & 2) && r.s1 == 1.0) ||
+                      ((s.pole_sides & 4) && r.t0 == 0.0) || ((s.pole_sides & 8) && r.t1 == 1.0);
+    if (!pole) {
       double3 r = e.p - p;
       double gs = dot(r, e.ps), gt = dot(r, e.pt), gl = sqrt(gs * gs + gt * gt);
       if (gl > 0.0 && rect_no_critical(box, d1, p, gs / gl, gt / gl)) continue;

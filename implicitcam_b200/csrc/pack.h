@@ -47,7 +47,10 @@ struct DNurbs {
 struct DSub {
   int32_t face, nurbs, span_a, span_b;
   int32_t klass;  // trim class of its parameter rectangle: 1 wholly inside, -1 straddles
-  int32_t pad;
+  // its sides on a side of the face's domain that the surface collapses on to one point
+  // (a pole): bit 0 s = 0, 1 s = 1, 2 t = 0, 3 t = 1; a part of it touching one is never
+  // cleared by the critical-point test (surface3.rs:579-591 Creases)
+  int32_t pole_sides;
   double u0, u1, v0, v1;  // its rectangle in the face's parameters
   double box[6];          // control-point box
   double c[3];            // rebasing origin (box centre)
@@ -86,6 +89,8 @@ struct DPiece {
   double uv[2][2][2];   // [side][end][u,v]
 };
 
+// A point feature with its pseudo-normal: the solid's vertices (angle-weighted), then
+// its B-spline faces' poles (a collapsed side's point, the fan pseudo-normal).
 struct DVert {
   double p[3];
   double pn[3];

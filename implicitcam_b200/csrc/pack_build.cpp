@@ -49,15 +49,82 @@ struct SpanGrid {
   std::vector<Bicubic> spans;
   int nsu, nsv;
 };
+// The face's domain, from its spans: u in [u0, u1], v in [v0, v1].
+void grid_domain(const SpanGrid& g, double* u0, double* u1, double* v0, double* v1) {
+  *u0 = g.spans.front().u0, *v0 = g.spans.front().v0;
+  *u1 = g.spans[size_t(g.nsu - 1) * g.nsv].u1, *v1 = g.spans[size_t(g.nsv - 1)].v1;
+}
+
+// The surface at global (u, v), with its derivatives along the span's own parameters.
+void grid_eval(const SpanGrid& g, double u, double v, V* P, V* Ps, V* Pt, V* Pst) {
+  int a = 0, b = 0;
+  while (a + 1 < g.nsu && g.spans[size_t(a + 1) * g.nsv].u0 <= u) a++;
+  while (b + 1 < g.nsv && g.spans[size_t(b + 1)].v0 <= v) b++;
+  const Bicubic& sp = g.spans[size_t(a) * g.nsv + b];
+  const double s = std::min(std::max((u - sp.u0) / (sp.u1 - sp.u0), 0.0), 1.0);
+  const double t = std::min(std::max((v - sp.v0) / (sp.v1 - sp.v0), 0.0), 1.0);
+  V Pss, Ptt;
+  sp.eval(s, t, P, Ps, Pt, &Pss, Pst, &Ptt);
+}
+
+// A side of a B-spline face's domain that its surface collapses on to one point (a
+// pole's side): k 0 when u is held (at `value`), the point x.
+struct Collapsed {
+  int k;
+  double value;
+  V x;
+};
+
+// surface3.rs:1392-1413 collapsed_sides: the domain sides along which 17 evenly spaced
+// points of the surface lie within 1e-12 of its control box's diagonal of the first.
+std::vector<Collapsed> collapsed_sides(const SpanGrid& g) {
+  Bx bx;
+  for (auto& sp : g.spans) bx.add(sp.box());
+  const double scale = std::max((bx.hi - bx.lo).len(), 1e-9);
+  double u0, u1, v0, v1;
+  grid_domain(g, &u0, &u1, &v0, &v1);
+  std::vector<Collapsed> out;
+  for (int k = 0; k < 2; k++) {
+    const double o0 = k == 0 ? v0 : u0, o1 = k == 0 ? v1 : u1;
+    for (double side : k == 0 ? std::vector<double>{u0, u1} : std::vector<double>{v0, v1}) {
+      auto at = [&](double w) {
+        V P, Ps, Pt, Pst;
+        if (k == 0)
+          grid_eval(g, side, w, &P, &Ps, &Pt, &Pst);
+        else
+          grid_eval(g, w, side, &P, &Ps, &Pt, &Pst);
+        return P;
+      };
+      const V x = at(o0);
+      bool same = true;
+      for (int i = 1; i <= 16 && same; i++)
+        if ((at(o0 + (o1 - o0) * i / 16.0) - x).len() > 1e-12 * scale) same = false;
+      if (same) out.push_back({k, side, x});
+    }
+  }
+  return out;
+}
+
+// Whether local (s0, t0) of span (a, b) lies on one of the face's collapsed sides.
+bool on_collapsed(const SpanGrid& g, const std::vector<Collapsed>& cs, int a, int b, double s0, double t0) {
+  const Bicubic& sp = g.spans[size_t(a) * g.nsv + b];
+  const double u = s0 == 0.0 ? sp.u0 : (s0 == 1.0 ? sp.u1 : sp.u0 + s0 * (sp.u1 - sp.u0));
+  const double v = t0 == 0.0 ? sp.v0 : (t0 == 1.0 ? sp.v1 : sp.v0 + t0 * (sp.v1 - sp.v0));
+  for (auto& c : cs)
+    if ((c.k == 0 ? u : v) == c.value) return true;
+  return false;
+}
+
 // A B-spline face's creases: the interior span boundaries across which the spans' unit
 // normals differ (sampled at five points a span; 1e-7), where the surface is only C0 and
 // folds (Exact::c0_line, solid3.rs:1821; the reference finds them by knots of full
 // multiplicity, a knot line with a continuous normal needs no feature of its own). Each
-// (k, a): the boundary before span a along u (k 0) or v (k 1). False, with the reason,
-// when a side of a span collapses to a point (a pole, solid3.rs:1609-1625): this pack
-// has no pole feature, so such a face is refused rather than packed with the pole's
-// nearest points missing.
-bool span_creases(const SpanGrid& g, std::vector<std::pair<int, int>>* creases, std::string* why) {
+// (k, a): the boundary before span a along u (k 0) or v (k 1). Samples on a collapsed
+// side (a pole's, where the normal is not defined) are skipped. False, with the reason,
+// when the normal vanishes anywhere else on a span's side: a degenerate point that no
+// feature of this pack covers.
+bool span_creases(const SpanGrid& g, const std::vector<Collapsed>& cs, std::vector<std::pair<int, int>>* creases,
+                  std::string* why) {
   auto normal = [](const Bicubic& sp, double s, double t, double* len) {
     V P, Ps, Pt, Pss, Pst, Ptt;
     sp.eval(s, t, &P, &Ps, &Pt, &Pss, &Pst, &Ptt);
@@ -66,17 +133,19 @@ bool span_creases(const SpanGrid& g, std::vector<std::pair<int, int>>* creases, 
     return n.unit();
   };
   const double ts[5] = {0.0, 0.25, 0.5, 0.75, 1.0};
-  for (auto& sp : g.spans)
-    for (double t : ts)
-      for (int side = 0; side < 4; side++) {
-        const double s0 = side == 0 ? 0.0 : (side == 1 ? 1.0 : t), t0 = side == 2 ? 0.0 : (side == 3 ? 1.0 : t);
-        double l;
-        normal(sp, s0, t0, &l);
-        if (!(l > 1e-9)) {
-          *why = "a side of its B-spline surface collapses to a point (a pole): not packed";
-          return false;
+  for (int a = 0; a < g.nsu; a++)
+    for (int b = 0; b < g.nsv; b++)
+      for (double t : ts)
+        for (int side = 0; side < 4; side++) {
+          const double s0 = side == 0 ? 0.0 : (side == 1 ? 1.0 : t), t0 = side == 2 ? 0.0 : (side == 3 ? 1.0 : t);
+          if (on_collapsed(g, cs, a, b, s0, t0)) continue;
+          double l;
+          normal(g.spans[size_t(a) * g.nsv + b], s0, t0, &l);
+          if (!(l > 1e-9)) {
+            *why = "its B-spline surface has no normal at a point off its collapsed sides: not packed";
+            return false;
+          }
         }
-      }
   for (int k = 0; k < 2; k++) {
     const int na = k == 0 ? g.nsu : g.nsv, nb = k == 0 ? g.nsv : g.nsu;
     for (int a = 1; a < na; a++) {
@@ -85,6 +154,7 @@ bool span_creases(const SpanGrid& g, std::vector<std::pair<int, int>>* creases, 
         const Bicubic& p0 = g.spans[k == 0 ? (a - 1) * g.nsv + b : b * g.nsv + a - 1];
         const Bicubic& p1 = g.spans[k == 0 ? a * g.nsv + b : b * g.nsv + a];
         for (double t : ts) {
+          if (k == 0 ? on_collapsed(g, cs, a, b, 0.0, t) : on_collapsed(g, cs, b, a, t, 0.0)) continue;
           double l0, l1;
           const V n0 = k == 0 ? normal(p0, 1.0, t, &l0) : normal(p0, t, 1.0, &l0);
           const V n1 = k == 0 ? normal(p1, 0.0, t, &l1) : normal(p1, t, 0.0, &l1);
@@ -230,6 +300,7 @@ bool build_pack(const IcamSolidDesc* d, double need, HostPack* hp, std::string* 
   // ---------------------------------------------------------------- faces and spans
   std::vector<SpanGrid> grids(d->n_faces);
   std::vector<std::vector<std::pair<int, int>>> creases(d->n_faces);
+  std::vector<std::vector<Collapsed>> collapsed(d->n_faces);
   std::vector<TrimTree> trees(d->n_faces);
   for (int fi = 0; fi < d->n_faces; fi++) {
     const IcamFaceDesc& fd = d->faces[fi];
@@ -297,7 +368,8 @@ bool build_pack(const IcamSolidDesc* d, double need, HostPack* hp, std::string* 
             }
         }
       std::string why;
-      if (!span_creases(grids[fi], &creases[fi], &why)) {
+      collapsed[fi] = collapsed_sides(grids[fi]);
+      if (!span_creases(grids[fi], collapsed[fi], &creases[fi], &why)) {
         *err = "face " + std::to_string(fi) + ": " + why;
         return false;
       }
@@ -599,6 +671,12 @@ bool build_pack(const IcamSolidDesc* d, double need, HostPack* hp, std::string* 
           s.span_b = b;
           s.klass = klass;
           s.u0 = sp.u0, s.u1 = sp.u1, s.v0 = sp.v0, s.v1 = sp.v1;
+          for (auto& c : collapsed[fi]) {
+            if (c.k == 0 && sp.u0 == c.value) s.pole_sides |= 1;
+            if (c.k == 0 && sp.u1 == c.value) s.pole_sides |= 2;
+            if (c.k == 1 && sp.v0 == c.value) s.pole_sides |= 4;
+            if (c.k == 1 && sp.v1 == c.value) s.pole_sides |= 8;
+          }
           for (int c = 0; c < 3; c++) s.box[c] = bx.lo[c], s.box[3 + c] = bx.hi[c];
           V mid = bx.mid();
           s.c[0] = mid.x, s.c[1] = mid.y, s.c[2] = mid.z;
@@ -665,6 +743,57 @@ bool build_pack(const IcamSolidDesc* d, double need, HostPack* hp, std::string* 
     v.pn[0] = pn[i].x, v.pn[1] = pn[i].y, v.pn[2] = pn[i].z;
     P.verts.push_back(v);
   }
+  // ---------------------------------------------------------------- poles (solid3.rs:1615-1625)
+  // A collapsed side's point at no vertex, with the side's middle inside the face, is a
+  // point feature packed after the vertices: its distance and its sign by the fan
+  // pseudo-normal (solid3.rs:1960-1986) times the face's sense. Near the point the surface
+  // is the cone of its limiting tangents S_k(w), with limiting normals S_k x S_kw (u held)
+  // or S_kw x S_v (v held), oriented as S_u x S_v just inside; each pair of neighbouring
+  // samples (513 along the side) whose side is covered by the face (the trim tested 1e-9
+  // of the domain into it) adds its mean normal times the angle its tangent turns through.
+  for (int fi = 0; fi < d->n_faces; fi++)
+    for (auto& c : collapsed[fi]) {
+      bool at_vertex = false;
+      for (int i = 0; i < d->n_verts; i++)
+        if ((V(d->verts[3 * i], d->verts[3 * i + 1], d->verts[3 * i + 2]) - c.x).len() <= d->tol) at_vertex = true;
+      if (at_vertex) continue;
+      const SpanGrid& g = grids[fi];
+      double u0, u1, v0, v1;
+      grid_domain(g, &u0, &u1, &v0, &v1);
+      const double r0 = c.k == 0 ? u0 : v0, r1 = c.k == 0 ? u1 : v1;
+      const double o0 = c.k == 0 ? v0 : u0, o1 = c.k == 0 ? v1 : u1;
+      auto inside = [&](double along, double w) {
+        return c.k == 0 ? trees[fi].inside(along, w) : trees[fi].inside(w, along);
+      };
+      if (!inside(c.value, 0.5 * (o0 + o1))) continue;
+      const double h = c.value == r0 ? 1.0 : -1.0, step = 1e-9 * (r1 - r0) * h;
+      const int n = 512;
+      V out, ptan, pnrm;
+      bool have = false, pcov = false;
+      for (int i = 0; i <= n; i++) {
+        const double w = o0 + (o1 - o0) * i / double(n);
+        V Pp, Ps, Pt, Pst;
+        if (c.k == 0)
+          grid_eval(g, c.value, w, &Pp, &Ps, &Pt, &Pst);
+        else
+          grid_eval(g, w, c.value, &Pp, &Ps, &Pt, &Pst);
+        const V tan = (c.k == 0 ? Ps : Pt) * h;
+        const V nrm = (c.k == 0 ? Ps.cross(Pst) : Pst.cross(Pt)) * h;
+        const bool cov = inside(c.value + step, w);
+        if (have && pcov && cov && tan.len() > 0.0 && ptan.len() > 0.0) {
+          const V ta = ptan.unit(), tb = tan.unit();
+          const double ang = std::atan2(ta.cross(tb).len(), ta.dot(tb));
+          const V m = pnrm.unit() + nrm.unit();
+          if (m.len() > 0.0) out = out + m.unit() * ang;
+        }
+        ptan = tan, pnrm = nrm, pcov = cov, have = true;
+      }
+      const V fn = out * P.faces[fi].sense;
+      DVert v{};
+      v.p[0] = c.x.x, v.p[1] = c.x.y, v.p[2] = c.x.z;
+      v.pn[0] = fn.x, v.pn[1] = fn.y, v.pn[2] = fn.z;
+      P.verts.push_back(v);
+    }
   // ---------------------------------------------------------------- the tree over every feature
   std::vector<Item> items;
   Bx all;

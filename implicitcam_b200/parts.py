@@ -536,6 +536,49 @@ def dome(r=3.0, height=4.0):
     return b
 
 
+def nurbs_dome(r=3.0, height=4.0, rise=None):
+    """`dome` with its cap as a rational biquadratic B-spline of revolution: u the angle
+    about z (four quarter arcs, knots 0..4, periodic), v the meridian from the equator
+    (v = 0) to the apex (v = 1). rise None: the hemisphere (a quarter arc, the apex
+    smooth); else the meridian's control points (r, height), (r / 2, height + 3 rise / 4),
+    (0, height + rise), a pointed apex (a cone point). The equator is the cap's boundary
+    curve (a spline edge of four rational quadratic pieces). The side v = 1 collapses to
+    the apex, a pole inside the face (its one loop is the equator): the reference's pole
+    feature with its fan pseudo-normal (solid3.rs:1609-1625, 1960-1986) answers the points
+    whose nearest point it is."""
+    s = math.sqrt(0.5)
+    ring = [(1, 0, 1), (1, 1, s), (0, 1, 1), (-1, 1, s), (-1, 0, 1), (-1, -1, s), (0, -1, 1), (1, -1, s), (1, 0, 1)]
+    if rise is None:
+        merid = [(r, height, 1.0), (r, height + r, s), (0.0, height + r, 1.0)]
+    else:
+        merid = [(r, height, 1.0), (0.5 * r, height + 0.75 * rise, 1.0), (0.0, height + rise, 1.0)]
+    net = np.array([[[cx * rho * wu * wv, cy * rho * wu * wv, zz * wu * wv, wu * wv] for rho, zz, wv in merid]
+                    for cx, cy, wu in ring])
+    ku = [0.0] * 3 + [1.0, 1.0, 2.0, 2.0, 3.0, 3.0] + [4.0] * 3
+    kv = [0.0] * 3 + [1.0] * 3
+    patches, ub, vb_ = surface_spans(2, 2, ku, kv, net)
+    b = SolidBuilder(tol=1e-9)
+    z, x = [0, 0, 1], [1, 0, 0]
+    f0 = Frame([0, 0, 0], z, x)
+    va, vb = b.vertex([r, 0, 0]), b.vertex([r, 0, height])
+    c0 = b.arc(f0, r, 0.0, TAU, va, va)
+    c1 = b.spline(_boundary_pieces(patches, "v0"), vb, vb)
+    seam = b.line(va, vb)
+    _plane_face(b, f0, -1, [[(c0, True)]])
+    lo, hi = _pad([0.0, 0.0], [TAU, height])
+    cyl = b.face(CYLINDER, +1, f0, a=r, lo=[0.0, lo[1]], hi=[TAU, hi[1]], period=[TAU, 0.0])
+    b.loop(cyl, [
+        (c0, False, line_pcurve([0.0, 0.0], [TAU, 0.0])),
+        (seam, False, None),
+        (c1, True, line_pcurve([TAU, height], [0.0, height])),
+        (seam, True, None),
+    ])
+    cap = b.face(NURBS, +1, lo=[ub[0], vb_[0]], hi=[ub[-1], vb_[-1]], period=[ub[-1] - ub[0], 0.0],
+                 nurbs=(patches, ub, vb_))
+    b.loop(cap, [(c1, False, line_pcurve([ub[0], 0.0], [ub[-1], 0.0]))])
+    return b
+
+
 def _dome_body(b: SolidBuilder, cx, cy, z0, r, height):
     """A dome standing on the plane z = z0: a cylinder of radius r to z0 + height capped by
     the hemisphere on its top circle. Returns its base circle, a hole loop for the plane."""

@@ -169,6 +169,17 @@ void NurbsSurf::build_tree() {
   build(0, nsu, 0, nsv);
 }
 
+// surface3.rs:587-591 Creases::touches
+bool NurbsSurf::touches(const Patch& pa) const {
+  auto on = [](double x, const std::vector<double>& lines, double a, double b) {
+    for (double c : lines)
+      if (std::fabs(x - c) <= 1e-12 * std::max(std::fabs(b - a), std::fabs(c))) return true;
+    return false;
+  };
+  return on(pa.u0, cu, pa.u0, pa.u1) || on(pa.u1, cu, pa.u0, pa.u1) || on(pa.v0, cv, pa.v0, pa.v1) ||
+         on(pa.v1, cv, pa.v0, pa.v1);
+}
+
 // surface3.rs:1168-1173 span_of
 int NurbsSurf::span_of(const std::vector<double>& br, double x) const {
   int n = int(br.size()) - 1;
@@ -275,8 +286,9 @@ bool NurbsSurf::closest_trimmed(V3 p, double cutoff, const Trim2* trim, SurfHit*
     }
     double slab = slab_bound(pa, p, d > 1e-12 ? (p - e.p) * (1.0 / d) : n);
     if (slab >= best_d - DIST_EPS || it->depth >= 40) continue;
-    // no collapsed sides in these descriptions: the test applies to every patch
-    if (pa.no_critical_point(p)) continue;
+    // a patch touching a collapsed side is never cleared: the distance's minimum at a
+    // pole need not be a critical point of the patch's parameters
+    if (!touches(pa) && pa.no_critical_point(p)) continue;
     Patch q[4];
     pa.quarters(q);
     for (int k = 0; k < 4; k++) {
@@ -878,6 +890,65 @@ bool Exact::init(const IcamSolidDesc* d, std::string* err) {
     }
     boxes.push_back(b);
   }
+  // solid3.rs:1615-1625 poles: each side of a B-spline face's domain that its surface
+  // collapses on to one point (surface3.rs:1392-1413 collapsed_sides, 17 points along the
+  // side within 1e-12 of the surface's size) is a crease of its search; where the point is
+  // at no vertex and the side's middle is inside the face, a point feature with the fan
+  // pseudo-normal
+  poles.clear();
+  for (size_t fi = 0; fi < faces.size(); fi++) {
+    Face& f = faces[fi];
+    if (f.surf.kind != NURBS || !f.surf.ns) continue;
+    NurbsSurf& ns = *f.surf.ns;
+    Box sb = ns.bbox();
+    double scale = std::max((sb.second - sb.first).len(), 1e-9);
+    for (int k = 0; k < 2; k++) {
+      const std::vector<double>& rb = k == 0 ? ns.ub : ns.vb;
+      const std::vector<double>& ob = k == 0 ? ns.vb : ns.ub;
+      const double o0 = ob.front(), o1 = ob.back();
+      for (double side : {rb.front(), rb.back()}) {
+        auto at = [&](double w) { return k == 0 ? ns.eval(side, w) : ns.eval(w, side); };
+        V3 x = at(o0).p;
+        bool collapsed = true;
+        for (int i = 1; i <= 16 && collapsed; i++)
+          if ((at(o0 + (o1 - o0) * i / 16.0).p - x).len() > 1e-12 * scale) collapsed = false;
+        if (!collapsed) continue;
+        (k == 0 ? ns.cu : ns.cv).push_back(side);
+        bool at_vertex = false;
+        for (auto& v : verts)
+          if ((v.p - x).len() <= tol) at_vertex = true;
+        if (at_vertex) continue;
+        const double mid = 0.5 * (o0 + o1);
+        if (!(k == 0 ? f.trim.inside(side, mid) : f.trim.inside(mid, side))) continue;
+        // solid3.rs:1960-1986 fan_normal: near the point the surface is the cone of its
+        // limiting tangents S_k(w) with limiting normals S_k x S_kw (u held) or
+        // S_kw x S_v (v held), oriented as S_u x S_v just inside; each pair of
+        // neighbouring samples whose side is covered by the face adds its mean normal
+        // times the angle its tangent turns through
+        const double h = side == rb.front() ? 1.0 : -1.0;
+        const double step = 1e-9 * (rb.back() - rb.front()) * h;
+        const int n = 512;
+        V3 out, ptan, pnrm;
+        bool have = false, pcov = false;
+        for (int i = 0; i <= n; i++) {
+          const double w = o0 + (o1 - o0) * i / double(n);
+          SEval e = at(w);
+          V3 tan = (k == 0 ? e.ps : e.pt) * h;
+          V3 nrm = (k == 0 ? e.ps.cross(e.pst) : e.pst.cross(e.pt)) * h;
+          const bool cov = k == 0 ? f.trim.inside(side + step, w) : f.trim.inside(w, side + step);
+          if (have && pcov && cov && tan.len() > 0.0 && ptan.len() > 0.0) {
+            V3 a = ptan.unit(), c = tan.unit();
+            const double ang = std::atan2(a.cross(c).len(), a.dot(c));
+            V3 m = pnrm.unit() + nrm.unit();
+            if (m.len() > 0.0) out = out + m.unit() * ang;
+          }
+          ptan = tan, pnrm = nrm, pcov = cov, have = true;
+        }
+        poles.push_back({int(fi), x, out * f.sense});
+      }
+    }
+  }
+  for (auto& pl : poles) boxes.push_back({pl.x, pl.x});
   tree_.init(boxes);
   return true;
 }
@@ -1095,11 +1166,15 @@ Sd Exact::sdf_within(V3 p, double bound, ExactStats* st) const {
       const Vert& v = verts[vi];
       double d = (p - v.p).len();
       if (d < cur) best = {d * sign((p - v.p).dot(v.pn)), v.p, 2, int(vi), false};
-    } else {  // solid3.rs:1790-1795 a knot line
+    } else if (id < nF + nE + verts.size() + lines.size()) {  // solid3.rs:1790-1795 a knot line
       const C0Line& l = lines[id - nF - nE - verts.size()];
       double d;
       V3 q, n;
       if (c0_line(l, p, cur, st, &d, &q, &n)) best = {d * sign((p - q).dot(n)), q, 0, l.face, false};
+    } else {  // solid3.rs:1795-1801 a pole
+      const Pole& pl = poles[id - nF - nE - verts.size() - lines.size()];
+      double d = (p - pl.x).len();
+      if (d < cur) best = {d * sign((p - pl.x).dot(pl.n)), pl.x, 0, pl.face, false};
     }
     if (best.d != before) {
       found = true;
@@ -1128,6 +1203,8 @@ std::vector<size_t> Exact::candidates(V3 c, double r, double d) const {
       lb = e.kind <= 1 ? e.closest(c).dist : 0.0;
     } else if (id < nF + nE + verts.size()) {
       lb = (c - verts[id - nF - nE].p).len();
+    } else if (id >= nF + nE + verts.size() + lines.size()) {
+      lb = (c - poles[id - nF - nE - verts.size() - lines.size()].x).len();
     } else {
       lb = box_dist(c, tree_.boxes_of(id));
     }
@@ -1142,7 +1219,8 @@ int Exact::kind_of(size_t id) const {
   if (id < nf()) return faces[id].surf.kind == NURBS ? 1 : 0;
   if (id < nf() + ne()) return edges[id - nf()].curve.kind <= 1 ? 2 : 3;
   if (id < nf() + ne() + nv()) return 4;
-  return 3;  // a knot line: as a spline edge
+  if (id < nf() + ne() + nv() + lines.size()) return 3;  // a knot line: as a spline edge
+  return 4;                                              // a pole: as a vertex
 }
 
 // partcache.rs:962-970 packed

@@ -36,6 +36,11 @@ struct NurbsSurf {
     std::vector<int> kids;
   };
   std::vector<QNode> nodes;
+  // surface3.rs:579-591 Creases: the domain sides the surface collapses on to one point
+  // (u held at each of cu, v at each of cv); a patch with a side on one is never cleared
+  // by the critical-point test
+  std::vector<double> cu, cv;
+  bool touches(const Patch& pa) const;
   void build_tree();
   int build(int i0, int i1, int j0, int j1);
   const Patch& span(int a, int b) const { return spans[a * nsv + b]; }
@@ -178,6 +183,13 @@ struct C0Line {
   std::vector<const Patch*> before, after;
 };
 
+// solid3.rs:1551-1553 a pole: the point a B-spline face's side collapses on to, inside
+// the face and at no vertex, with the fan pseudo-normal (times the face's sense)
+struct Pole {
+  int face = 0;
+  V3 x, n;
+};
+
 class Exact {
  public:
   bool init(const IcamSolidDesc* d, std::string* err);
@@ -195,6 +207,7 @@ class Exact {
   std::vector<EdgeRec> edges;
   std::vector<Vert> verts;
   std::vector<C0Line> lines;  // the tree's ids after the vertices
+  std::vector<Pole> poles;    // the tree's ids after the knot lines
   Box bbox;
 
  private:
