@@ -595,6 +595,21 @@ HD bool is_critical(double3 p, const SE& e) {
   return fabs(dot(r, e.ps)) <= (round + 1e-12 * ls) * ls && fabs(dot(r, e.pt)) <= (round + 1e-12 * lt) * lt;
 }
 
+// The same with each tangent's rounding allowance raised by how much shorter than
+// `scale` (the part's size) the tangent is. Beside a pole the tangent along the
+// collapsing side is the difference of nearly equal control points, its direction
+// known only to about eps * scale / |S_s|, and the reference's allowance rejects the
+// nearest point there (its residual is that rounding); used for sub-patches with a
+// side on a pole's.
+HD bool is_critical_scaled(double3 p, const SE& e, double scale) {
+  double3 r = e.p - p;
+  double big = fmax(fmax(fabs(e.p.x), fabs(e.p.y)), fabs(e.p.z)) + fmax(fmax(fabs(p.x), fabs(p.y)), fabs(p.z));
+  double round = 1024.0 * 2.220446049250313e-16 * (big + len(r));
+  double ls = len(e.ps), lt = len(e.pt);
+  double rs = round * fmax(1.0, scale / ls), rt = round * fmax(1.0, scale / lt);
+  return fabs(dot(r, e.ps)) <= (rs + 1e-12 * ls) * ls && fabs(dot(r, e.pt)) <= (rt + 1e-12 * lt) * lt;
+}
+
 // Interval product.
 HD void imul(double alo, double ahi, double blo, double bhi, double* lo, double* hi) {
   double p0 = alo * blo, p1 = alo * bhi, p2 = ahi * blo, p3 = ahi * bhi;
@@ -607,7 +622,11 @@ HD void imul(double alo, double ahi, double blo, double bhi, double* lo, double*
 // eigenvalue is at least lam + min_i(E_ii - |E_12|) (Gershgorin) with E_ij the interval
 // of (S - p).S_ij over S in the control box and S_ij in their bounds
 // (surface3.rs:814-845 convex_radius, tightened by the offset box as gpu.wgsl:1547-1604).
+// Never for a sub-patch with a side on a pole's: the metric degenerates there, the
+// bound is at best semi-definite, and projected Newton can rest on the pole with the
+// nearest point a little inside; such a sub-patch is always searched by subdivision.
 HD bool sub_convex(const DSub& s, double3 plo, double3 phi) {
+  if (s.pole_sides != 0) return false;
   double dlo[3] = {s.box[0] - phi.x, s.box[1] - phi.y, s.box[2] - phi.z};
   double dhi[3] = {s.box[3] - plo.x, s.box[4] - plo.y, s.box[5] - plo.z};
   double elo[3], ehi[3];

@@ -175,7 +175,11 @@ HDI void bb_sub(const DPack& P, int si, double3 p, Acc& A) {
     }
     double lb = fmax(box_dist(p, box), r.lb);
     if (lb >= bound - DIST_EPS || lb > far) continue;
-    bool cert = rect_convex(box, lam, d2, p);
+    // a part touching a pole's side: never certified convex, never cleared by the
+    // critical-point test (the distance's minimum at the pole need not be critical)
+    const bool pole = ((s.pole_sides & 1) && r.s0 == 0.0) || ((s.pole_sides & 2) && r.s1 == 1.0) ||
+                      ((s.pole_sides & 4) && r.t0 == 0.0) || ((s.pole_sides & 8) && r.t1 == 1.0);
+    bool cert = !pole && rect_convex(box, lam, d2, p);
     double ss = 0.5, tt = 0.5;
     bool conv;
     newton_bicubic(q, p, &ss, &tt, cert ? 16 : 12, &conv);
@@ -188,18 +192,18 @@ HDI void bb_sub(const DPack& P, int si, double3 p, Acc& A) {
       if (s.klass == 1 || trim_inside(P, f, u, v)) {
         bound = d;
         A.ub = fmin(A.ub, d);
-        if (d < A.best && is_critical(p, e) && len(n) > 0.0) {
+        // beside a pole the tangent along the collapsing side is known only to the
+        // rounding of nearly equal control points: its allowance scales with the part
+        const bool crit = s.pole_sides ? is_critical_scaled(p, e, len(mk(box[3], box[4], box[5]) - mk(box[0], box[1], box[2])))
+                                       : is_critical(p, e);
+        if (d < A.best && crit && len(n) > 0.0) {
           double3 nn = unit(n) * f.sense;
           take(A, d, d * sgn(dot(p - e.p, nn)));
         }
       }
     }
     if (cert && conv) continue;  // its one minimum is known
-    // no critical point in the part: nothing of the face's is here (surface3.rs:1280-1282);
-    // a part touching a pole's side is never cleared (the distance's minimum at the pole
-    // need not be a critical point of the part's parameters)
-    const bool pole = ((s.pole_sides & 1) && r.s0 == 0.0) || ((s.pole_sides & 2) && r.s1 == 1.0) ||
-                      ((s.pole_sides & 4) && r.t0 == 0.0) || ((s.pole_sides & 8) && r.t1 == 1.0);
+    // no critical point in the part: nothing of the face's is here (surface3.rs:1280-1282)
     if (!pole) {
       double3 r = e.p - p;
       double gs = dot(r, e.ps), gt = dot(r, e.pt), gl = sqrt(gs * gs + gt * gt);

@@ -100,16 +100,18 @@ typedef struct IcamBakeStats {
  * crates/icam-core/src/solid3/gpu.rs:259). Returns ICAM_OK and *out, or an error
  * with a message in err. A B-spline face's creases (interior knot lines where its
  * normal jumps, Exact::c0_line, solid3.rs:1821-1886) are packed as the face's own
- * edges; ICAM_ERR_PACK, before any device work, for a crease that crosses its face's
- * loops or a side collapsed to a point (a pole: no pole feature is built, fan_normal,
- * solid3.rs:1960-1986). */
+ * edges; a side of a B-spline face's domain collapsed to one point inside the face
+ * (a pole, solid3.rs:1615-1625) is packed as a point feature with the fan
+ * pseudo-normal (fan_normal, solid3.rs:1960-1986), after the solid's vertices.
+ * ICAM_ERR_PACK, before any device work, for a crease that crosses its face's loops or
+ * a B-spline face whose normal vanishes off its collapsed sides. */
 int icam_pack_create(const IcamSolidDesc* solid, const IcamPackOptions* opt, IcamPack** out, char* err,
                      size_t errlen);
 
 void icam_pack_destroy(IcamPack* pack);
 
-/* Counts of what the pack holds: faces, edges, vertices, B-spline sub-patches,
- * edge pieces, trim cells, tree nodes. */
+/* Counts of what the pack holds: faces, edges, point features (vertices, then
+ * poles), B-spline sub-patches, edge pieces, trim cells, tree nodes. */
 int icam_pack_info(const IcamPack* pack, int64_t counts[7]);
 
 /* Signed distance of n points (x, y, z), each (value, flag) as above. With

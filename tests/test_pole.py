@@ -6,17 +6,18 @@ surface3.rs:579-591).
 CPU: with a pointed apex, the oracle's distances equal the closed form (the distance in the
 meridian plane to the profile: bottom, wall and the quadratic meridian), above the apex
 where the pole is the nearest point and everywhere around it; with the hemisphere, they
-equal the analytic dome's; the pack takes the face. B200: the library's points agree with
-the oracle with equal signs, and its levels are the oracle's (the map identical, i16
-words within one step, no sign flip).
+equal the analytic dome's; the pack takes the face. B200: the library's points equal the
+closed form (pointed apex) and agree with the oracle with equal signs, and its levels are
+the oracle's (the map identical, i16 words within one step, no sign flip).
 
 Where a point lies a hair outside the pointed apex's normal cone its nearest point is on
-the cap within ~1e-3 mm of the apex, where the surface's u-tangent all but vanishes: the
-search's capped Newton (surface3.rs:1214-1297, 12 steps) stops short of the critical-point
-test's tolerance there, its polish returns the same distance rounded up, and the search has
-already lowered its bound to that distance, so the pole answers, up to ~1e-7 mm farther.
-The oracle keeps that behaviour; such points are a sliver of the cone's edge, so the tests
-hold nearly every point to 1e-12 and every point to the north star's 1e-7 of the diagonal.
+the cap within ~1e-3 mm of the apex, where the surface's u-tangent all but vanishes and is
+known only to the rounding of nearly equal control points: the reference's critical-point
+test (surface3.rs:565-572) rejects the nearest point there, the search has already lowered
+its bound to that distance, and the pole answers, up to ~1e-7 mm farther. The oracle keeps
+that behaviour (such points are a sliver of the cone's edge: the tests hold nearly every
+point to 1e-12 and every point to the north star's 1e-7 of the diagonal); the library
+scales that test's allowance on sub-patches beside a pole and finds the nearest point.
 """
 import numpy as np
 import pytest
@@ -138,6 +139,8 @@ def test_poles_on_the_gpu(oracle_mod, rise):
         v, f = g.points(p)
         d = o.sdf(p)[0]
         assert (f == 0).all()
+        if rise is not None:
+            assert np.abs(v - profile_distance(p)).max() < 1e-9 * diag
         err = np.abs(v - d)
         assert (err < 1e-9 * diag).mean() > 0.99
         assert err.max() < 1e-7 * diag
