@@ -140,9 +140,10 @@ int icam_bricks(IcamPack* pack, const double* first_nodes, size_t n, double h, d
  * calls on that device share: calls that overlap in time race on it. n above
  * ICAM_STATIC_BRICKS is refused with ICAM_ERR_ROOM; ICAM_MIXED_LEARNED on a pack
  * whose seed network is neither trained nor loaded with ICAM_ERR_ARG, as icam_bricks
- * refuses it. The call returns once the results are in values_out / d_out. The first
- * call on a device resolves the array's address and may load the library's device
- * code: make it before any stream capture. The address is kept until the process
+ * refuses it. The call is synchronous: it returns once the results are in values_out
+ * / d_out (host memory), so it may never be made while a stream of the device is
+ * being captured. The first call on a device resolves the array's address and may
+ * load the library's device code. The address is kept until the process
  * exits, so no call may follow a cudaDeviceReset of that device. Errors are written
  * to err (errlen bytes), not to the pack's message. */
 #define ICAM_STATIC_BRICKS 256
