@@ -368,7 +368,7 @@ int decide_level(IcamPack* pk, const LevelDesc& L, DecideOut* out) {
     }
     CK(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), s));
     launch_decide(a, s, is_first, L.precision != ICAM_FP64);
-    launches += is_first ? 2 : 1;
+    launches += is_first ? 3 : 1;
     CK(cudaGetLastError());
     unsigned long long nn = 0;
     CK(cudaMemcpyAsync(&nn, cnt, sizeof(nn), cudaMemcpyDeviceToHost, s));

@@ -466,7 +466,7 @@ __device__ __forceinline__ void box_geometry(const DecideArgs& a, const Box4& b,
 // neighbours until none changes (at most n sweeps); a box then known fills its map
 // entries; one no neighbour reached (no box of the level read exactly within its chain)
 // is read without a bound and decided as any other.
-__device__ void first_signs(const DecideArgs& a, int64_t n) {
+__device__ void first_signs(const DecideArgs& a, int64_t n, bool fill = true) {
   const long long fx = a.first_dims[0], fy = a.first_dims[1], fz = a.first_dims[2];
   volatile int8_t* sg = a.first_sign;
   __shared__ int changed;
@@ -504,6 +504,7 @@ __device__ void first_signs(const DecideArgs& a, int64_t n) {
     const int8_t si = sg[i];
     const Box4 b = a.boxes[i];
     if (si == FS_AIR || si == FS_SOLID) {
+      if (!fill) continue;  // k_first_fill writes them over the whole grid
       const uint32_t val = si == FS_AIR ? 0xffffffffu : 0xfffffffeu;
       for (long long z = max(b.z, 0LL); z < min(b.z + a.size, nb2); z++)
         for (long long y = max(b.y, 0LL); y < min(b.y + a.size, nb1); y++)
@@ -519,7 +520,26 @@ __device__ void first_signs(const DecideArgs& a, int64_t n) {
   }
 }
 
-__global__ void __launch_bounds__(256) k_first_signs(DecideArgs a, int64_t n) { first_signs(a, n); }
+__global__ void __launch_bounds__(256) k_first_signs(DecideArgs a, int64_t n) { first_signs(a, n, false); }
+
+// The map entries of the first boxes whose sign k_first_signs found (most of a level's
+// volume, far from the part): one thread a brick over the whole grid instead of the
+// sweep's single block.
+__global__ void __launch_bounds__(256) k_first_fill(DecideArgs a, int64_t n) {
+  const long long s = a.size, per = s * s * s;
+  const long long nb0 = a.nb[0], nb1 = a.nb[1], nb2 = a.nb[2];
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n * per;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int64_t i = t / per;
+    const int8_t si = a.first_sign[i];
+    if (si != FS_AIR && si != FS_SOLID) continue;
+    const long long k = t - i * per;
+    const Box4 b = a.boxes[i];
+    const long long x = b.x + k % s, y = b.y + (k / s) % s, z = b.z + k / (s * s);
+    if (x < 0 || y < 0 || z < 0 || x >= nb0 || y >= nb1 || z >= nb2) continue;
+    a.map[x + nb0 * (y + nb1 * z)] = si == FS_AIR ? 0xffffffffu : 0xfffffffeu;
+  }
+}
 
 // The boxes a warp takes together: 32 when there are enough groups of 32 to fill the
 // GPU's warp slots (two 4-warp blocks an SM), else fewer (down to 4), so that a round of
@@ -634,7 +654,12 @@ void launch_decide(const DecideArgs& a, cudaStream_t s, bool first, bool mixed) 
   } else {
     k_decide_w<<<grid, DWARPS * 32, 0, s>>>(a, gs);
   }
-  if (first) k_first_signs<<<1, 256, 0, s>>>(a, a.n);
+  if (first) {
+    k_first_signs<<<1, 256, 0, s>>>(a, a.n);
+    const long long work = a.n * a.size * a.size * a.size;
+    const int fg = int(std::max<long long>(1, std::min<long long>((work + 255) / 256, (long long)sms * 8)));
+    k_first_fill<<<fg, 256, 0, s>>>(a, a.n);
+  }
 }
 
 void launch_decide_batch(const DecideBatchArgs& b, int rounds, cudaStream_t s) {
