@@ -6,7 +6,8 @@ the centre, so a box that the tighter bound decides AIR (SOLID) holds only nodes
 clamp: the reference reads those bricks and packs each as an AIR (SOLID) brick (on a
 closed solid, whose signed distance changes by at most the distance moved). These CPU
 tests run the oracle's decision under both bounds and read every brick each one lists:
-the final maps and atlases are the same, and the tighter bound reads fewer bricks.
+the final maps and atlases are the same, and the tighter bound reads fewer bricks
+(a freeform top, bosses, a creased ridge and a pointed pole).
 """
 import numpy as np
 import pytest
@@ -37,9 +38,10 @@ def _bodies():
                                                      faces=6), 0.25, 1.0
     yield "bosses", parts.bodies_on_plate(seed=5, kind="boss", count=2, plate=(24.0, 12.0, 4.0)), 0.2, 0.2 * np.sqrt(3)
     yield "ridge", parts.ridge_box(fold=0.5, size=20.0, base=8.0, wave=0.4, n=7), 0.2, 0.6
+    yield "pole", parts.nurbs_dome(3.0, 4.0, rise=2.0), 0.1, 0.5
 
 
-@pytest.mark.parametrize("case", list(range(3)))
+@pytest.mark.parametrize("case", list(range(4)))
 def test_tight_bound_gives_the_same_level(oracle_mod, case):
     name, b, h, clamp = list(_bodies())[case]
     o = oracle_mod.Oracle(b)
