@@ -44,10 +44,10 @@ BAND = 2.0
 # leg; 6 Newton steps of 750 + trim 200; closed-form foot; 6 steps of 120; a distance
 FLOPS_PER_CANDIDATE = np.array([80.0, 6 * 750.0 + 200.0, 40.0, 6 * 120.0, 10.0])
 # DRAM bytes the brick kernel moves a read brick: one ncu capture of the same kernel
-# (mixed form) on the same part's level at h = 0.2 mm, 7x smaller (dram__bytes_read.sum
-# 12.51 MB + dram__bytes_write.sum 102.30 MB over 129,053 read bricks), scaled by the
-# bricks read
-TRAFFIC_PER_READ_BRICK = (12.513024e6 + 102.296832e6) / 129053
+# (mixed + learned) on the same part's level at h = 0.2 mm, 7x smaller (dram__bytes_read.sum
+# 19.39 MB + dram__bytes_write.sum 49.57 MB over the 74,588 bricks that bake reads),
+# scaled by the bricks read
+TRAFFIC_PER_READ_BRICK = (19.390720e6 + 49.571328e6) / 74588
 # the seed network's training: 50M pairs from the exact evaluator, before any timing
 SEEDNET_STEPS, SEEDNET_BATCH = 12208, 4096
 
