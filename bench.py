@@ -96,6 +96,21 @@ def newton_figures(st):
 FLOPS_PER_FLOAT_EVAL = 700.0
 
 
+def hbm_figure(traffic, node_ms):
+    """The brick kernel's DRAM traffic over its time against the measured copy bandwidth
+    (MEASURED_PEAKS.json hbm_gbs): the path is not bound by HBM; reported beside the
+    FP32/FP64 roofline."""
+    peak = None
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak = float(json.load(f)["hbm_gbs"])
+    except (OSError, KeyError, ValueError):
+        pass
+    gbs = traffic / (node_ms * 1e-3) / 1e9
+    return {"achieved_gbs": gbs, "peak_gbs": peak, "frac": gbs / peak if peak else None,
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peak else None}
+
+
 def executed_roofline(st, node_ms, peak):
     """The work the mixed walk did in the bake: its float patch evaluations (counted by
     the kernel) at FLOPS_PER_FLOAT_EVAL each, over the node phase's time, against the
@@ -434,7 +449,8 @@ def main():
                          "traffic_source": "ncu dram bytes of k_bricks at h = 0.2 mm, scaled by bricks read",
                          "peak_source": "measured FMA probe of this run (MEASURED_PEAKS.json holds no FP64/FP32 figure)",
                          "algorithmic_flops_per_launch": flops,
-                         "executed": executed_roofline(st, node_ms, peak)},
+                         "executed": executed_roofline(st, node_ms, peak),
+                         "hbm": hbm_figure(TRAFFIC_PER_READ_BRICK * st["bricks_read"], node_ms)},
             "cpu_baseline": cpu,
             "clocks": clocks,
         }
