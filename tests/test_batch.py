@@ -11,7 +11,8 @@ pytestmark = pytest.mark.gpu
 
 
 def uneven_parts():
-    """Planes, cylinders and rational B-spline tops of uneven sizes and face counts."""
+    """Planes, cylinders and rational B-spline tops of uneven sizes and face counts, and a
+    cap of revolution with a pole at its apex (its level's nodes kept off the axis)."""
     return [
         (parts.can(), 0.25, 0.25 * np.sqrt(3)),
         (parts.block_with_hole(), 1.0, np.sqrt(3)),
@@ -19,6 +20,7 @@ def uneven_parts():
         (parts.bump_box(), 0.125, 0.125 * np.sqrt(3)),
         (parts.freeform_top(seed=3, n=8, size=40.0, base=20.0, bumps=4), 0.25, 1.0),
         (parts.freeform_top(seed=5, n=12, size=60.0, base=30.0, bumps=6), 0.4, 2.0),
+        (parts.nurbs_dome(3.0, 4.0, rise=2.0), 0.1, 0.5, 0.0371),
     ]
 
 
@@ -30,10 +32,10 @@ def batch(oracle_mod):
         pytest.skip("no GPU")
     spec = uneven_parts()
     gs, levels = [], []
-    for solid, h, clamp in spec:
+    for solid, h, clamp, *shift in spec:
         g = part_gpu.PartGpu(solid)
         lo, hi = oracle_mod.Oracle(solid).bbox()
-        lo2 = np.asarray(lo) - 2.0
+        lo2 = np.asarray(lo) - 2.0 - (shift[0] if shift else 0.0)
         nb = np.ceil((np.asarray(hi) - np.asarray(lo) + 4.0) / (8 * h)).astype(np.int64)
         gs.append(g)
         levels.append((h, lo2, nb, clamp))
