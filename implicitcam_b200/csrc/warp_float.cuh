@@ -1,6 +1,6 @@
 // The mixed form's node walk: a warp's lanes query nodes of one brick over the brick's
 // ranked candidate list in single precision, every coordinate relative to the brick's
-// centre (and a sub-patch's net to its own centre), as the north star's bulk step:
+// centre (and a sub-patch's net to its own centre), the mixed precision's bulk step:
 // planes and B-spline sub-patches in floats; the rare features (edges, pieces, vertices,
 // curved faces) and the trim tests near loops in double precision out of line; and a
 // node whose float answer cannot be trusted (near zero, where the sign is decided; a

@@ -1,7 +1,7 @@
 """The CUDA library against the oracle and the golden vectors, on a B200.
 
 Tolerances: signed distances in double precision agree within 1e-9 of the part's box
-diagonal (the north star's bar for the plain FP64 kernel); signs, flags, the brick map
+diagonal (the bar for the plain FP64 kernel); signs, flags, the brick map
 and every packed atlas word agree exactly.
 """
 import os

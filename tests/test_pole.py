@@ -16,7 +16,7 @@ known only to the rounding of nearly equal control points: the reference's criti
 test (surface3.rs:565-572) rejects the nearest point there, the search has already lowered
 its bound to that distance, and the pole answers, up to ~1e-7 mm farther. The oracle keeps
 that behaviour (such points are a sliver of the cone's edge: the tests hold nearly every
-point to 1e-12 and every point to the north star's 1e-7 of the diagonal); the library
+point to 1e-12 and every point to the bake's 1e-7 of the diagonal); the library
 scales that test's allowance on sub-patches beside a pole and finds the nearest point.
 """
 import numpy as np
