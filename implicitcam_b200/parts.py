@@ -14,6 +14,8 @@
 - ``boss`` (cylinder, torus fillet, plane cap), ``countersunk_block`` (a hole with a
   cone countersink) and ``dome`` (a cylinder under a hemisphere): the analytic families
   of a batch of uneven parts;
+- ``nurbs_dome``, ``nurbs_ball``: a dome and a sphere whose caps are rational B-spline
+  surfaces of revolution collapsing at their poles;
 - ``mold``: a 250 x 200 x 80 mm block with a pocket whose floor is 500 one-span bicubic
   rational B-spline faces joined along shared B-spline edges, and 40 filleted bosses on
   its rim.
@@ -576,6 +578,24 @@ def nurbs_dome(r=3.0, height=4.0, rise=None):
     cap = b.face(NURBS, +1, lo=[ub[0], vb_[0]], hi=[ub[-1], vb_[-1]], period=[ub[-1] - ub[0], 0.0],
                  nurbs=(patches, ub, vb_))
     b.loop(cap, [(c1, False, line_pcurve([ub[0], 0.0], [ub[-1], 0.0]))])
+    return b
+
+
+def nurbs_ball(r=3.0):
+    """`ball` as one rational biquadratic B-spline face of revolution with no loops: u the
+    angle about z (four quarter arcs, periodic), v the meridian from the south pole
+    (v = 0) to the north pole (v = 2) in two quarter arcs. Both v sides collapse to a
+    point inside the face: two poles and no vertex."""
+    s = math.sqrt(0.5)
+    ring = [(1, 0, 1), (1, 1, s), (0, 1, 1), (-1, 1, s), (-1, 0, 1), (-1, -1, s), (0, -1, 1), (1, -1, s), (1, 0, 1)]
+    merid = [(0.0, -r, 1.0), (r, -r, s), (r, 0.0, 1.0), (r, r, s), (0.0, r, 1.0)]
+    net = np.array([[[cx * rho * wu * wv, cy * rho * wu * wv, zz * wu * wv, wu * wv] for rho, zz, wv in merid]
+                    for cx, cy, wu in ring])
+    ku = [0.0] * 3 + [1.0, 1.0, 2.0, 2.0, 3.0, 3.0] + [4.0] * 3
+    kv = [0.0] * 3 + [1.0, 1.0] + [2.0] * 3
+    patches, ub, vb = surface_spans(2, 2, ku, kv, net)
+    b = SolidBuilder(tol=1e-9)
+    b.face(NURBS, +1, lo=[ub[0], vb[0]], hi=[ub[-1], vb[-1]], period=[ub[-1] - ub[0], 0.0], nurbs=(patches, ub, vb))
     return b
 
 

@@ -6,7 +6,8 @@ surface3.rs:579-591).
 CPU: with a pointed apex, the oracle's distances equal the closed form (the distance in the
 meridian plane to the profile: bottom, wall and the quadratic meridian), above the apex
 where the pole is the nearest point and everywhere around it; with the hemisphere, they
-equal the analytic dome's; the pack takes the face. B200: the library's points equal the
+equal the analytic dome's; a sphere made of one such face with a pole at each end and no
+loops equals the analytic ball; the pack takes the faces. B200: the library's points equal the
 closed form (pointed apex) and agree with the oracle with equal signs, and its levels are
 the oracle's (the map identical, i16 words within one step, no sign flip).
 
@@ -88,13 +89,27 @@ def test_round_apex_is_the_analytic_dome(oracle_mod):
     assert not dn[4].any()
 
 
+def test_two_poles_are_the_ball(oracle_mod):
+    """A sphere as one B-spline face with no loops collapsing at both poles."""
+    a = oracle_mod.Oracle(parts.ball(R))
+    n = oracle_mod.Oracle(parts.nurbs_ball(R))
+    rng = np.random.default_rng(2)
+    p = np.concatenate([rng.uniform(-5, 5, (2000, 3)), np.array([0, 0, R]) + rng.normal(0, 0.3, (1000, 3)),
+                        np.array([0, 0, -R]) + rng.normal(0, 0.3, (1000, 3))])
+    p = p[np.hypot(p[:, 0], p[:, 1]) > 1e-3]
+    da, dn = a.sdf(p), n.sdf(p)
+    assert np.abs(da[0] - dn[0]).max() < 1e-11
+    assert (np.sign(da[0]) == np.sign(dn[0])).all()
+    assert not dn[4].any()
+
+
 def test_a_pole_face_packs():
     """The pack takes a face with a pole (the point feature and the never-cleared sides)
     before any device work; on a machine without a GPU the call then fails for want of
     one, not for the pole."""
-    for rise in (None, RISE):
+    for solid in (parts.nurbs_dome(R, H), parts.nurbs_dome(R, H, rise=RISE), parts.nurbs_ball(R)):
         try:
-            part_gpu.PartGpu(parts.nurbs_dome(R, H, rise=rise)).close()
+            part_gpu.PartGpu(solid).close()
         except part_gpu.IcamError as e:
             assert "no normal" not in str(e) and "B-spline" not in str(e)
 
@@ -113,6 +128,25 @@ def _oracle_level(o, h, lo, nb, clamp):
             if kind[j] == 0:
                 atlas.append(words[j])
     return m, np.array(atlas, dtype=np.uint32).reshape(-1, 365)
+
+
+@pytest.mark.gpu
+def test_two_poles_on_the_gpu(oracle_mod):
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no GPU")
+    g = part_gpu.PartGpu(parts.nurbs_ball(R), need=1.0)
+    try:
+        rng = np.random.default_rng(4)
+        p = np.concatenate([rng.uniform(-5, 5, (4000, 3)), np.array([0, 0, R]) + rng.normal(0, 0.3, (2000, 3)),
+                            np.array([0, 0, -R]) + rng.normal(0, 0.3, (2000, 3))])
+        p = p[np.hypot(p[:, 0], p[:, 1]) > 0.05]
+        v, f = g.points(p)
+        assert (f == 0).all()
+        assert np.abs(v - (np.linalg.norm(p, axis=1) - R)).max() < 1e-9 * 2 * R * np.sqrt(3)
+    finally:
+        g.close()
 
 
 @pytest.mark.gpu
