@@ -309,6 +309,11 @@ long long first_boxes(const LevelDesc& L, std::vector<Box4>* out, long long dims
   return size;
 }
 
+// The decision's device counters: 0 unused, 1 bricks to read, 2 centres read again in
+// double, then one box count a size from kSizeSlot on (at most 4 sizes and their end).
+constexpr int kSizeSlot = 4;
+constexpr int kCounts = kSizeSlot + 8;
+
 int decide_level(IcamPack* pk, const LevelDesc& L, DecideOut* out) {
   const double h = L.h, clamp = L.clamp;
   const double* lo = L.lo;
@@ -326,9 +331,9 @@ int decide_level(IcamPack* pk, const LevelDesc& L, DecideOut* out) {
   int64_t box_cap = std::max<int64_t>(total + 64, 1 << 12);
   if ((r = scratch(pk, 3, total * sizeof(uint32_t), &d_map)) || (r = scratch(pk, 4, box_cap * sizeof(Box4), &d_cur)) ||
       (r = scratch(pk, 5, box_cap * sizeof(Box4), &d_next)) || (r = scratch(pk, 6, total * sizeof(int64_t), &d_ridx)) ||
-      (r = scratch(pk, 7, total * sizeof(double), &d_rdc)) || (r = scratch(pk, 8, 4 * sizeof(unsigned long long), &d_cnt)))
+      (r = scratch(pk, 7, total * sizeof(double), &d_rdc)) || (r = scratch(pk, 8, kCounts * sizeof(unsigned long long), &d_cnt)))
     return r;
-  CK(cudaMemsetAsync(d_cnt, 0, 4 * sizeof(unsigned long long), s));
+  CK(cudaMemsetAsync(d_cnt, 0, kCounts * sizeof(unsigned long long), s));
   std::vector<Box4> first;
   long long dims[3];
   long long size = first_boxes(L, &first, dims);
@@ -339,53 +344,57 @@ int decide_level(IcamPack* pk, const LevelDesc& L, DecideOut* out) {
   out->d2h_bytes = 0;
   int64_t ncur = int64_t(first.size()), boxes_read = 0;
   unsigned long long* cnt = (unsigned long long*)d_cnt;
-  while (ncur > 0) {
+  // One launch a box size (size, size / 2, ..., 1), back to back: size k's boxes are the
+  // ones size k - 1 appended, counted in slot kSizeSlot + k on the device, which the
+  // kernels read themselves (the first size's count is the host's); the host reads the
+  // counts back once, after the last size.
+  int rounds = 0;
+  for (long long s2 = size; s2 >= 1; s2 /= 2) rounds++;
+  if (kSizeSlot + rounds + 1 > kCounts) return fail(pk, ICAM_ERR_ARG, "too many box sizes");
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  for (int k = 0; k < rounds; k++) {
     DecideArgs a{};
     a.P = pk->dev;
     a.leaves = pk->leaves;
     a.n_leaves = int32_t(pk->leaves_host.size());
-    a.boxes = (const Box4*)d_cur;
-    a.n = ncur;
-    a.size = size;
+    a.boxes = (const Box4*)(k % 2 == 0 ? d_cur : d_next);
+    a.n = k == 0 ? ncur : box_cap;
+    a.n_in = k == 0 ? nullptr : cnt + kSizeSlot + k;
+    a.sms = sms;
+    a.size = size >> k;
     a.h = h;
     a.clamp = clamp;
-    for (int k = 0; k < 3; k++) a.lo[k] = lo[k], a.nb[k] = nb[k];
+    for (int q = 0; q < 3; q++) a.lo[q] = lo[q], a.nb[q] = nb[q];
     a.map = (uint32_t*)d_map;
-    a.next = (Box4*)d_next;
+    a.next = (Box4*)(k % 2 == 0 ? d_next : d_cur);
     a.next_cap = box_cap;
-    a.n_next = cnt + 0;
+    a.n_next = cnt + kSizeSlot + k + 1;
     a.read_idx = (int64_t*)d_ridx;
     a.read_dc = (double*)d_rdc;
     a.read_cap = total;
     a.n_read = cnt + 1;
-    const bool is_first = launches == 0;
     a.n_double = cnt + 2;
     a.tight = L.tight ? 1 : 0;
-    if (is_first) {
+    if (k == 0) {
       a.first_sd = static_cast<double*>(d_first);
       a.first_sign = reinterpret_cast<int8_t*>(static_cast<double*>(d_first) + ncur);
-      for (int k = 0; k < 3; k++) a.first_dims[k] = dims[k];
+      for (int q = 0; q < 3; q++) a.first_dims[q] = dims[q];
     }
-    CK(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), s));
-    launch_decide(a, s, is_first, L.precision != ICAM_FP64);
-    launches += is_first ? 3 : 1;
+    launch_decide(a, s, k == 0, L.precision != ICAM_FP64);
+    launches += k == 0 ? 3 : 1;
     CK(cudaGetLastError());
-    unsigned long long nn = 0;
-    CK(cudaMemcpyAsync(&nn, cnt, sizeof(nn), cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    out->d2h_bytes += sizeof(nn);
-    boxes_read += ncur;
-    if (int64_t(nn) > box_cap) return fail(pk, ICAM_ERR_ROOM, "box list overflow");
-    std::swap(d_cur, d_next);
-    ncur = int64_t(nn);
-    size /= 2;
   }
-  unsigned long long nread = 0;
-  unsigned long long cnt_host[4] = {0, 0, 0, 0};
+  unsigned long long cnt_host[kCounts] = {};
   CK(cudaMemcpyAsync(cnt_host, cnt, sizeof(cnt_host), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   out->d2h_bytes += sizeof(cnt_host);
-  nread = cnt_host[1];
+  boxes_read = ncur;
+  for (int k = 1; k <= rounds; k++) {
+    if (cnt_host[kSizeSlot + k] > (unsigned long long)box_cap) return fail(pk, ICAM_ERR_ROOM, "box list overflow");
+    if (k < rounds) boxes_read += int64_t(cnt_host[kSizeSlot + k]);
+  }
+  const unsigned long long nread = cnt_host[1];
   out->centres_double = int64_t(cnt_host[2]);
   const int64_t R = int64_t(nread);
   // the read bricks in brick order (partcache.rs:486)

@@ -550,11 +550,24 @@ __host__ __device__ inline int group_size(int64_t n, int sms) {
   return gs;
 }
 
-__global__ void __launch_bounds__(DWARPS * 32, 2) k_decide_w(DecideArgs a, int gs) {
+// This size's box count and group size: the launch's, or read from the device.
+__device__ __forceinline__ void round_count(const DecideArgs& a, int gs_launch, int64_t* n, int* gs) {
+  *n = a.n;
+  *gs = gs_launch;
+  if (a.n_in) {
+    *n = min(int64_t(*a.n_in), a.n);
+    *gs = group_size(*n, a.sms);
+  }
+}
+
+__global__ void __launch_bounds__(DWARPS * 32, 2) k_decide_w(DecideArgs a, int gs_launch) {
   __shared__ DecideSmem smem[DWARPS];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int64_t g0 = (int64_t(blockIdx.x) * DWARPS + warp) * gs; g0 < a.n; g0 += int64_t(gridDim.x) * DWARPS * gs)
-    decide_group(a, a.boxes, a.n, a.size, g0, gs, smem[warp], lane, a.first_sd != nullptr);
+  int64_t n;
+  int gs;
+  round_count(a, gs_launch, &n, &gs);
+  for (int64_t g0 = (int64_t(blockIdx.x) * DWARPS + warp) * gs; g0 < n; g0 += int64_t(gridDim.x) * DWARPS * gs)
+    decide_group(a, a.boxes, n, a.size, g0, gs, smem[warp], lane, a.first_sd != nullptr);
 }
 
 // The mixed form's decision of one box size: three blocks a SM (the float walk's
@@ -569,13 +582,16 @@ __device__ __forceinline__ void decide_f_init(DecideSmemF& S, int lane) {
   __syncwarp();
 }
 
-__global__ void __launch_bounds__(DWARPS * 32, ICAM_MIXED_BLOCKS) k_decide_wf(DecideArgs a, int gs) {
+__global__ void __launch_bounds__(DWARPS * 32, ICAM_MIXED_BLOCKS) k_decide_wf(DecideArgs a, int gs_launch) {
   extern __shared__ __align__(16) unsigned char dsm[];
   DecideSmemF* smem = reinterpret_cast<DecideSmemF*>(dsm);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   decide_f_init(smem[warp], lane);
-  for (int64_t g0 = (int64_t(blockIdx.x) * DWARPS + warp) * gs; g0 < a.n; g0 += int64_t(gridDim.x) * DWARPS * gs)
-    decide_group_f(a, a.boxes, a.n, a.size, g0, gs, smem[warp], lane, a.first_sd != nullptr);
+  int64_t n;
+  int gs;
+  round_count(a, gs_launch, &n, &gs);
+  for (int64_t g0 = (int64_t(blockIdx.x) * DWARPS + warp) * gs; g0 < n; g0 += int64_t(gridDim.x) * DWARPS * gs)
+    decide_group_f(a, a.boxes, n, a.size, g0, gs, smem[warp], lane, a.first_sd != nullptr);
 }
 
 // A batch's round (one box size a part): the counts the last round appended become this
@@ -645,7 +661,7 @@ void launch_decide(const DecideArgs& a, cudaStream_t s, bool first, bool mixed) 
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int per_sm = mixed ? ICAM_MIXED_BLOCKS : 2;
   const int gs = group_size(a.n, sms);
-  const int64_t want = (a.n + DWARPS * gs - 1) / (DWARPS * gs);
+  const int64_t want = a.n_in ? int64_t(sms) * per_sm : (a.n + DWARPS * gs - 1) / (DWARPS * gs);
   const int grid = int(std::max<int64_t>(1, std::min<int64_t>(want, int64_t(sms) * per_sm)));
   if (mixed) {
     const size_t smem = sizeof(DecideSmemF) * DWARPS;
@@ -654,7 +670,7 @@ void launch_decide(const DecideArgs& a, cudaStream_t s, bool first, bool mixed) 
   } else {
     k_decide_w<<<grid, DWARPS * 32, 0, s>>>(a, gs);
   }
-  if (first) {
+  if (first) {  // the first size's count is the host's (n_in unset)
     k_first_signs<<<1, 256, 0, s>>>(a, a.n);
     const long long work = a.n * a.size * a.size * a.size;
     const int fg = int(std::max<long long>(1, std::min<long long>((work + 255) / 256, (long long)sms * 8)));

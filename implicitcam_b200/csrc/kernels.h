@@ -68,7 +68,12 @@ struct DecideArgs {
   const int32_t* leaves;  // the tree's leaf nodes
   int32_t n_leaves;
   const Box4* boxes;
-  int64_t n;
+  int64_t n;  // the boxes; with n_in, the most the list holds
+  // when set, the count of boxes the previous size appended (read on the device, capped
+  // at n), so that sizes follow one another without the host reading counts back; the
+  // launch then spans the whole GPU (sms multiprocessors) and groups are sized on it
+  const unsigned long long* n_in;
+  int32_t sms;
   long long size;
   double h, clamp;
   double lo[3];
