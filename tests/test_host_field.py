@@ -47,13 +47,13 @@ def host_lib(tmp_path_factory):
     return lib
 
 
-def host_points(lib, solid, p, need=2.0):
+def host_points(lib, solid, p, need=2.0, cap=np.inf):
     desc = solid.desc()
     p = np.ascontiguousarray(p, dtype=np.float64)
     v = np.zeros(len(p))
     f = np.zeros(len(p), np.int32)
     err = C.create_string_buffer(512)
-    rc = lib.host_points(C.addressof(desc), need, p.ctypes.data, len(p), np.inf, v.ctypes.data, f.ctypes.data, err,
+    rc = lib.host_points(C.addressof(desc), need, p.ctypes.data, len(p), cap, v.ctypes.data, f.ctypes.data, err,
                          512)
     assert rc == 0, err.value
     return v, f
@@ -97,3 +97,24 @@ def test_device_search_on_the_host(oracle_mod, host_lib, name):
         assert err.max() < 1e-9 * diag
     sure = np.abs(d) > 1e-9
     assert (np.sign(v[sure]) == np.sign(d[sure])).all()
+
+
+@pytest.mark.parametrize("name", ["block_with_hole", "freeform_top", "ridge", "pointed_pole"])
+def test_capped_reads_on_the_host(oracle_mod, host_lib, name):
+    """A read capped at 1 mm (the decision's and the brick lists' reads): exact with flag
+    0 within the cap, the cap with flag 1 past it (gpu.wgsl:1909-1921)."""
+    solid = CASES[name]()
+    o = oracle_mod.Oracle(solid)
+    lo, hi = map(np.asarray, o.bbox())
+    diag = float(np.linalg.norm(hi - lo))
+    rng = np.random.default_rng(9)
+    p = rng.uniform(lo - 2.0, hi + 2.0, (1500, 3))
+    if "pole" in name:
+        p = p[np.hypot(p[:, 0], p[:, 1]) > 0.05]
+    cap = 1.0
+    v, f = host_points(host_lib, solid, p, cap=cap)
+    d = o.sdf(p)[0]
+    inner, outer = np.abs(d) < cap - 1e-9, np.abs(d) > cap + 1e-9
+    assert inner.sum() > 50 and outer.sum() > 50
+    assert (f[inner] == 0).all() and np.abs(v[inner] - d[inner]).max() < 1e-7 * diag
+    assert (f[outer] == 1).all() and (v[outer] == cap).all()
